@@ -1,0 +1,196 @@
+/*
+ * ppvm_cuda.h — C ABI of the B200 Pauli-propagation engine.
+ *
+ * This is the drop-in boundary for the Heisenberg-picture PauliSum hot path of
+ * QuEraComputing/ppvm.  Every entry point below names the reference interface it
+ * replaces (paths are relative to the ppvm repository).  The reference binds this
+ * path through PyO3 (`crates/ppvm-python-native/src/interface.rs`); a Rust crate
+ * or a Python ctypes shim binds these symbols instead.
+ *
+ * Conventions
+ *  - A Pauli word over n qubits is two bit planes of W = ceil(n/64) u64 words:
+ *    qubit q is bit (q % 64) of word (q / 64) of the X plane and of the Z plane.
+ *    I=(0,0) X=(1,0) Z=(0,1) Y=(1,1), as `PauliWord` stores it
+ *    (`crates/ppvm-pauli-word/src/word/data.rs:43-52`, Lsb0 bit order).
+ *  - Host arrays of words are term-major: x[k*W + w].  Bits at or above n must be 0.
+ *  - Coefficients are IEEE binary64.
+ *  - Every call returns a ppvm_status; no call aborts the process.  The text of the
+ *    last error on the calling thread is available from ppvm_last_error_string().
+ *  - A handle owns its device buffers and one CUDA stream.  Calls on one handle
+ *    are serialised by the caller (the reference's `&mut self`); different handles
+ *    may be driven from different threads.
+ *  - Gate calls with `truncate != 0` run the handle's truncation strategy once
+ *    after the whole target list, as the PyO3 binding does
+ *    (`interface.rs:156-310`: `<gate>_many(targets)` then `truncate()`).
+ */
+#ifndef PPVM_CUDA_H
+#define PPVM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ppvm_status {
+  PPVM_OK = 0,
+  PPVM_EINVAL = 1,    /* bad argument (odd pair list, qubit out of range, ...) */
+  PPVM_ECAPACITY = 2, /* device memory exhausted / size limit exceeded */
+  PPVM_ECUDA = 3,     /* a CUDA runtime call failed */
+  PPVM_ETIMEOUT = 4,  /* a bounded device-side wait gave up */
+  PPVM_ENODEV = 5     /* no usable CUDA device */
+} ppvm_status;
+
+typedef struct ppvm_sum ppvm_sum; /* opaque */
+
+/* Operation codes of a gate list (ppvm_gate_list_run). */
+typedef enum ppvm_opcode {
+  PPVM_OP_X = 0, PPVM_OP_Y, PPVM_OP_Z, PPVM_OP_H, PPVM_OP_S, PPVM_OP_S_DAG,
+  PPVM_OP_SQRT_X, PPVM_OP_SQRT_X_DAG, PPVM_OP_SQRT_Y, PPVM_OP_SQRT_Y_DAG,
+  PPVM_OP_CNOT, PPVM_OP_CZ, PPVM_OP_CY,                  /* q0 = control, q1 = target */
+  PPVM_OP_RX, PPVM_OP_RY, PPVM_OP_RZ,                    /* angle in theta */
+  PPVM_OP_RXX, PPVM_OP_RYY, PPVM_OP_RZZ,                 /* q0, q1, theta */
+  PPVM_OP_PAULI_ERROR,                                   /* q0, p[0..2] = (px, py, pz) */
+  PPVM_OP_DEPOLARIZE1,                                   /* q0, theta = p */
+  PPVM_OP_DEPOLARIZE2,                                   /* q0, q1, theta = p */
+  PPVM_OP_TRUNCATE,                                      /* run the strategy */
+  PPVM_OP_COUNT_
+} ppvm_opcode;
+
+typedef struct ppvm_op {
+  uint32_t code;  /* ppvm_opcode */
+  uint32_t q0;
+  uint32_t q1;
+  uint32_t flags; /* reserved, 0 */
+  double theta;
+  double p[3];
+} ppvm_op;
+
+/* Sum creation options (bit flags for ppvm_sum_create2). */
+#define PPVM_FLAG_CLIFFORD_ANGLES 1u /* treat Pauli rotations at theta = +-pi/2 as the
+                                        Clifford they equal (cos = 0, sin = +-1 exactly) */
+
+/* ---- lifetime ------------------------------------------------------------------ */
+
+/* PauliSum::builder().n_qubits(n).strategy(CombinedStrategy(CoefficientThreshold(min_abs_coeff),
+ * MaxPauliWeight(max_weight))).capacity(..).build()  (crates/ppvm-pauli-sum/src/sum/data.rs:65-91,
+ * strategy built as in crates/ppvm-python-native/src/interface.rs:51-57,78-98).
+ * max_weight = UINT64_MAX disables the weight cap (crates/ppvm-pauli-sum/src/strategy.rs:86-88).
+ * capacity_hint = initial term capacity (0 = a small default); storage grows on demand. */
+ppvm_status ppvm_sum_create(ppvm_sum** out, uint32_t n_qubits, double min_abs_coeff,
+                            uint64_t max_weight, size_t capacity_hint);
+/* As ppvm_sum_create, plus option flags (PPVM_FLAG_*) and a device ordinal. */
+ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_coeff,
+                             uint64_t max_weight, size_t capacity_hint, uint32_t flags,
+                             int device);
+/* Drop (data.rs:40 `PauliSum` owns both maps). NULL is accepted. */
+ppvm_status ppvm_sum_destroy(ppvm_sum* sum);
+/* Clone (data.rs:40 derive(Clone); interface.rs:373-375 __copy__): device-to-device copy. */
+ppvm_status ppvm_sum_clone(const ppvm_sum* src, ppvm_sum** out);
+/* Bind the handle to a caller-owned cudaStream_t (NULL = the handle's own stream). */
+ppvm_status ppvm_sum_set_stream(ppvm_sum* sum, void* cuda_stream);
+
+/* ---- terms --------------------------------------------------------------------- */
+
+/* `ps += (word, c)` for each of k terms, in order (crates/ppvm-pauli-sum/src/sum/ops.rs:140-151
+ * -> IndexMap entry().and_modify(+=).or_insert, crates/ppvm-traits/src/map/hashmap.rs:40-44). */
+ppvm_status ppvm_sum_add_terms(ppvm_sum* sum, const uint64_t* x, const uint64_t* z,
+                               const double* c, size_t k);
+/* Same for one Pauli string "IXYZ..." of length n ('_' skipped as in word/data.rs:332-377). */
+ppvm_status ppvm_sum_add_string(ppvm_sum* sum, const char* word, double c);
+/* preserve_strings of the builder (data.rs:75-77, restore logic data.rs:283-310). */
+ppvm_status ppvm_sum_set_preserve(ppvm_sum* sum, const uint64_t* x, const uint64_t* z, size_t k);
+
+/* len() (data.rs:165-167; interface.rs:389-391). */
+ppvm_status ppvm_len(const ppvm_sum* sum, size_t* out);
+/* terms() (interface.rs:393-395): copies up to cap terms in the sum's iteration order. */
+ppvm_status ppvm_export_terms(const ppvm_sum* sum, uint64_t* x, uint64_t* z, double* c,
+                              size_t cap, size_t* n_out);
+/* weights() / current_max_weight() (interface.rs:397-403; PauliWord::weight, word/data.rs:150-182). */
+ppvm_status ppvm_weights(const ppvm_sum* sum, uint32_t* w, size_t cap, size_t* n_out);
+ppvm_status ppvm_current_max_weight(const ppvm_sum* sum, uint64_t* out);
+/* __eq__ (data.rs:345-352): same n_qubits and same key->value map (order-free). */
+ppvm_status ppvm_equal(const ppvm_sum* a, const ppvm_sum* b, int* out);
+
+/* ---- Clifford gates (crates/ppvm-pauli-sum/src/sum/clifford.rs:37-221) ----------- */
+/* Single-qubit: targets[k]; CliffordBatch `*_many` loops (crates/ppvm-traits/src/traits/clifford.rs:175-258). */
+ppvm_status ppvm_x(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_y(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_z(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_h(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_s(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_s_dag(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_sqrt_x(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_sqrt_x_dag(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_sqrt_y(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+ppvm_status ppvm_sqrt_y_dag(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+/* Two-qubit: flat (control, target) pairs; odd k_flat -> PPVM_EINVAL
+ * (crates/ppvm-python-native/src/lib.rs:12-22 flat_pairs). */
+ppvm_status ppvm_cnot(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, int truncate);
+ppvm_status ppvm_cz(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, int truncate);
+ppvm_status ppvm_cy(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, int truncate);
+
+/* ---- rotations (crates/ppvm-pauli-sum/src/sum/rot1.rs:44-143, rot2.rs:12-184) ----- */
+ppvm_status ppvm_rx(ppvm_sum* sum, const uint32_t* targets, size_t k, double theta, int truncate);
+ppvm_status ppvm_ry(ppvm_sum* sum, const uint32_t* targets, size_t k, double theta, int truncate);
+ppvm_status ppvm_rz(ppvm_sum* sum, const uint32_t* targets, size_t k, double theta, int truncate);
+/* RotXY::r = rz(phi); rx(theta); rz(-phi) (rot1.rs:131-143; interface.rs:281-285). */
+ppvm_status ppvm_r(ppvm_sum* sum, uint32_t q, double axis_angle, double theta, int truncate);
+ppvm_status ppvm_rxx(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, double theta, int truncate);
+ppvm_status ppvm_ryy(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, double theta, int truncate);
+ppvm_status ppvm_rzz(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, double theta, int truncate);
+/* Generic Pauli rotation exp(-i theta/2 G), G given by its X/Z planes (W words each).
+ * Generalises RotationOne::rotate_1 (rot1.rs:49-52) and RotationTwo::rotate_2 (rot2.rs:17-60)
+ * to any support: commuting P is unchanged; anticommuting P -> cos(theta) P + sin(theta) iGP. */
+ppvm_status ppvm_pauli_rotation(ppvm_sum* sum, const uint64_t* gx, const uint64_t* gz,
+                                double theta, int truncate);
+
+/* ---- noise channels (crates/ppvm-pauli-sum/src/sum/noise.rs) ------------------------ */
+/* PauliError::pauli_error (noise.rs:17-37), p = (px, py, pz); pauli_error_many loops. */
+ppvm_status ppvm_pauli_error(ppvm_sum* sum, const uint32_t* targets, size_t k, const double p[3],
+                             int truncate);
+/* Depolarizing::depolarize1 / depolarize2 (noise.rs:107-129). */
+ppvm_status ppvm_depolarize1(ppvm_sum* sum, const uint32_t* targets, size_t k, double p, int truncate);
+ppvm_status ppvm_depolarize2(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, double p,
+                             int truncate);
+
+/* ---- truncation, readout ---------------------------------------------------------- */
+/* PauliSum::truncate (data.rs:275-311) with CombinedStrategy(CoefficientThreshold, MaxPauliWeight)
+ * (crates/ppvm-pauli-sum/src/strategy.rs:12-30,73-90,125-134). */
+ppvm_status ppvm_truncate(ppvm_sum* sum);
+/* overlap_with_zero() = trace("Z?*") (interface.rs:122-130): sum of c over words without X bits. */
+ppvm_status ppvm_overlap_with_zero(ppvm_sum* sum, double* out);
+/* <0..0| O |0..0> of the propagated observable; the same quantity as overlap_with_zero. */
+ppvm_status ppvm_expectation(ppvm_sum* sum, double* out);
+/* trace(pattern) (interface.rs:122-126) for the PauliPattern grammar of
+ * crates/ppvm-pauli-word/src/pattern/parse.rs:32-127, matched as pattern/contains.rs:120-151. */
+ppvm_status ppvm_trace(ppvm_sum* sum, const char* pattern, double* out);
+/* PauliSum::overlap (crates/ppvm-pauli-sum/src/sum/trace.rs:31-37): sum_k a[k] * b[k]. */
+ppvm_status ppvm_overlap(ppvm_sum* a, ppvm_sum* b, double* out);
+
+/* ---- fused gate lists ---------------------------------------------------------------- */
+/* Runs ops[0..n_ops) in order; PPVM_OP_TRUNCATE marks where the strategy runs.  Consecutive
+ * Clifford ops are fused into one device pass.  Equivalent to calling the per-gate
+ * functions above with truncate = 0 plus ppvm_truncate at each TRUNCATE op. */
+ppvm_status ppvm_gate_list_run(ppvm_sum* sum, const ppvm_op* ops, size_t n_ops);
+/* Number of live terms entering each op of the last ppvm_gate_list_run (the numerator of
+ * the term-gate-updates metric); cap entries are written, n_out = n_ops of that run. */
+ppvm_status ppvm_last_run_live_counts(const ppvm_sum* sum, uint64_t* counts, size_t cap,
+                                      size_t* n_out);
+
+/* ---- diagnostics ------------------------------------------------------------------- */
+/* Thread-local text of the last failing call ("" if none). */
+const char* ppvm_last_error_string(void);
+/* Device time per kernel family, accumulated while profiling is on (CUDA events on the
+ * handle's stream).  names: NUL-separated list written to `names` (cap bytes). */
+ppvm_status ppvm_profile_enable(ppvm_sum* sum, int on);
+ppvm_status ppvm_profile_read(ppvm_sum* sum, char* names, size_t names_cap, double* ms,
+                              uint64_t* launches, uint64_t* bytes, size_t cap, size_t* n_out);
+/* Library version string. */
+const char* ppvm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PPVM_CUDA_H */

@@ -1,0 +1,107 @@
+"""Gate-list encoding shared by the host API, the workload generators and the tests.
+
+The opcodes mirror ``ppvm_opcode`` in include/ppvm_cuda.h.  A gate is a tuple
+``(code, q0, q1, theta, (p0, p1, p2))``; helpers below build them.
+
+Pauli words are held as two bit planes of ``W = ceil(n/64)`` u64 words, qubit ``q`` at
+bit ``q % 64`` of word ``q // 64`` (the Lsb0 layout of ``PauliWord``,
+crates/ppvm-pauli-word/src/word/data.rs:43-52 in the reference).
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+X, Y, Z, H, S, S_DAG, SQRT_X, SQRT_X_DAG, SQRT_Y, SQRT_Y_DAG = range(10)
+CNOT, CZ, CY = 10, 11, 12
+RX, RY, RZ = 13, 14, 15
+RXX, RYY, RZZ = 16, 17, 18
+PAULI_ERROR, DEPOLARIZE1, DEPOLARIZE2 = 19, 20, 21
+TRUNCATE = 22
+
+NAMES = {
+    X: "x", Y: "y", Z: "z", H: "h", S: "s", S_DAG: "s_dag", SQRT_X: "sqrt_x",
+    SQRT_X_DAG: "sqrt_x_dag", SQRT_Y: "sqrt_y", SQRT_Y_DAG: "sqrt_y_dag", CNOT: "cnot",
+    CZ: "cz", CY: "cy", RX: "rx", RY: "ry", RZ: "rz", RXX: "rxx", RYY: "ryy", RZZ: "rzz",
+    PAULI_ERROR: "pauli_error", DEPOLARIZE1: "depolarize1", DEPOLARIZE2: "depolarize2",
+    TRUNCATE: "truncate",
+}
+SINGLE_CLIFFORD = {X, Y, Z, H, S, S_DAG, SQRT_X, SQRT_X_DAG, SQRT_Y, SQRT_Y_DAG}
+TWO_CLIFFORD = {CNOT, CZ, CY}
+ROT1 = {RX, RY, RZ}
+ROT2 = {RXX, RYY, RZZ}
+HALF_PI = math.pi / 2
+
+_ZERO3 = (0.0, 0.0, 0.0)
+
+
+def g1(code: int, q: int):
+    return (code, q, 0, 0.0, _ZERO3)
+
+
+def g2(code: int, a: int, b: int):
+    return (code, a, b, 0.0, _ZERO3)
+
+
+def r1(code: int, q: int, theta: float):
+    return (code, q, 0, float(theta), _ZERO3)
+
+
+def r2(code: int, a: int, b: int, theta: float):
+    return (code, a, b, float(theta), _ZERO3)
+
+
+def pauli_error(q: int, p):
+    return (PAULI_ERROR, q, 0, 0.0, tuple(float(v) for v in p))
+
+
+def truncate():
+    return (TRUNCATE, 0, 0, 0.0, _ZERO3)
+
+
+def words(n_qubits: int) -> int:
+    return (n_qubits + 63) // 64
+
+
+def parse_word(s: str, n_qubits: int | None = None):
+    """Pauli string -> (x[W], z[W]) u64 planes; '_' is skipped like the reference parser
+    (crates/ppvm-pauli-word/src/word/data.rs:332-377)."""
+    chars = [c for c in s if c != "_"]
+    n = len(chars) if n_qubits is None else n_qubits
+    if len(chars) != n:
+        raise ValueError(f"word {s!r} has {len(chars)} qubits, expected {n}")
+    W = words(n)
+    x = np.zeros(W, dtype=np.uint64)
+    z = np.zeros(W, dtype=np.uint64)
+    for q, c in enumerate(chars):
+        b = np.uint64(1) << np.uint64(q % 64)
+        if c == "X":
+            x[q // 64] |= b
+        elif c == "Z":
+            z[q // 64] |= b
+        elif c == "Y":
+            x[q // 64] |= b
+            z[q // 64] |= b
+        elif c != "I":
+            raise ValueError(f"Invalid Pauli character: {c}")
+    return x, z
+
+
+def word_str(x, z, n_qubits: int) -> str:
+    out = []
+    for q in range(n_qubits):
+        xb = (int(x[q // 64]) >> (q % 64)) & 1
+        zb = (int(z[q // 64]) >> (q % 64)) & 1
+        out.append("IXZY"[xb | (zb << 1)])
+    return "".join(out)
+
+
+def weight(x, z) -> int:
+    return int(sum(bin(int(a) | int(b)).count("1") for a, b in zip(x, z)))
+
+
+def reverse_heisenberg(forward):
+    """Heisenberg order is the exact reverse of the forward gate list."""
+    return list(reversed(forward))
