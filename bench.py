@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark of the Heisenberg-picture PauliSum path on B200.
+
+Metric: term-gate updates/s = sum over the gates of a circuit of the live terms entering
+each gate (reference semantics: merge after every gate, truncate at the list's TRUNCATE ops),
+divided by the time.  A step is one complete propagation of the observable through the
+workload's gate list plus the <O> readout.
+
+Workload (default): 2D kicked Ising on an open 12x12 lattice, 20 layers, RX(0.6) on every
+qubit then RZZ(-pi/2) on all 264 bonds per layer, observable Z at (6,6), |c| < 1e-5
+truncation and weight cap 10, FP64 coefficients, synthetic inputs (the circuit is generated).
+
+Arms:
+  default           the CUDA engine through its C ABI (ppvm_b200.PauliSum)
+  --impl reference  the CPU restatement of the reference PauliSum (oracle/) on the host,
+                    on a bounded layer prefix of the same workload (rank 0 only)
+
+Multi-GPU (torchrun): every rank propagates its own replica of the circuit (the path has
+no cross-sum exchange at one sum per GPU); value = all ranks' updates / max rank time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from ppvm_b200 import circuits as C  # noqa: E402
+from ppvm_b200 import gates as G  # noqa: E402
+
+METRIC = "term-gate updates/s"
+CPU_PREFIX_LAYERS = 7  # bounded CPU sample: the first 7 Heisenberg layers (~10-20 s single thread)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ppvm_b200", choices=["ppvm_b200", "reference"])
+    ap.add_argument("--layers", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(layers: int):
+    return C.kicked_ising_2d(L=12, layers=layers, theta_h=0.6, thr=1e-5, max_weight=10)
+
+
+def config_dict(wl, n_gpus, extra=None):
+    d = {"workload": f"kicked_ising_2d 12x12 open lattice, {wl.meta['layers']} layers, RX(0.6) + RZZ(-pi/2) "
+                     f"on 264 bonds, obs Z(6,6), thr 1e-5, weight cap 10",
+         "n_qubits": wl.n_qubits, "gates_per_step": wl.n_gates, "layers": wl.meta["layers"],
+         "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single sum"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------------------------
+def oracle_run(wl):
+    from oracle.pyoracle import OracleSum
+
+    o = OracleSum(wl.n_qubits, wl.min_abs_coeff, wl.max_weight, wl.clifford_angles)
+    x, z = G.parse_word(wl.observable[0][0], wl.n_qubits)
+    o.add_terms(x[None], z[None], np.array([wl.observable[0][1]]))
+    t = time.perf_counter()
+    cnt = o.run_ops(wl.ops, counts=True)
+    val = o.overlap_with_zero()
+    dt = time.perf_counter() - t
+    return C.term_gate_updates(cnt, wl.ops), dt, val
+
+
+def cpu_baseline(layers: int):
+    wl = workload(min(layers, CPU_PREFIX_LAYERS))
+    tgu, dt, _ = oracle_run(wl)
+    return {"value": tgu / dt, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"first {wl.meta['layers']} Heisenberg layers of the workload, one propagation, "
+                      f"single-thread C++ restatement of the reference IndexMap PauliSum ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl = workload(min(args.layers, CPU_PREFIX_LAYERS))
+    for _ in range(args.warmup):
+        oracle_run(wl)
+    tot_u, tot_t = 0, 0.0
+    for _ in range(args.steps):
+        u, dt, _ = oracle_run(wl)
+        tot_u += u
+        tot_t += dt
+    v = tot_u / tot_t
+    line = {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (generated circuit)",
+            "config": config_dict(wl, 1, {"note": "bounded layer prefix of the workload on the host CPU"}),
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": "port",
+                             "sample": f"first {wl.meta['layers']} Heisenberg layers per step"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._loop, daemon=True)
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in self.rows for j in range(4) if len(r) > 5 + j and r[5 + j] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    from ppvm_b200.paulisum import PauliSum
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    wl = workload(args.layers)
+    obs_word, obs_c = wl.observable[0]
+
+    def make(capacity=0):
+        s = PauliSum([obs_word], wl.n_qubits, [obs_c], min_abs_coeff=wl.min_abs_coeff,
+                     max_pauli_weight=wl.max_weight, clifford_angles=True, device=local, capacity=capacity)
+        s.set_stream(stream.cuda_stream)
+        return s
+
+    # warm-up: also learns the peak live count so timed steps never grow storage
+    peak = 0
+    for _ in range(max(args.warmup, 1)):
+        s = make(peak * 2)
+        s.run(wl.ops)
+        s.overlap_with_zero()
+        counts = s.live_counts()
+        peak = max(peak, int(counts.max()), len(s))
+        del s
+    updates = C.term_gate_updates(counts, wl.ops)
+    cap = max(4 * peak, 1 << 16)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    # ---- device-resident timing: inputs already in HBM (sums created up front) -----------
+    sums = [make(cap) for _ in range(args.steps)]
+    for s in sums:
+        s.profile(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    results = []
+    with ClockSampler(local) as clk:
+        t_wall = time.perf_counter()
+        for i, s in enumerate(sums):
+            flush.fill_(float(i))
+            ev[i][0].record(stream)
+            s.run(wl.ops)
+            results.append(s.overlap_with_zero())
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    dev_s = sum(step_ms) / 1e3
+    prof = {}
+    for s in sums:
+        for k, v in s.profile_read().items():
+            p = prof.setdefault(k, {"ms": 0.0, "launches": 0, "bytes": 0})
+            p["ms"] += v["ms"]
+            p["launches"] += v["launches"]
+            p["bytes"] += v["bytes"]
+    del sums
+
+    # ---- end to end through the public API with host buffers ---------------------------------
+    e2e_ms = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        s = make(cap)  # host observable -> device
+        s.run(wl.ops)  # host gate list -> device, live-count log back
+        v = s.overlap_with_zero()  # result back to host
+        e2e_ms.append(1e3 * (time.perf_counter() - t))
+        del s
+    e2e_s = sum(e2e_ms) / 1e3
+    n_ops = len(wl.ops)
+    h2d = (16 * G.words(wl.n_qubits) + 8) + 40 * n_ops
+    d2h = 8 + 32 * n_ops
+
+    # ---- max over ranks ----------------------------------------------------------------------
+    t_dev = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
+    dev_s, e2e_s = float(t_dev[0]), float(t_dev[1])
+    total_updates = updates * args.steps * world
+    value = total_updates / dev_s
+    e2e_value = total_updates / e2e_s
+
+    if rank == 0:
+        peak_gbs, peak_kind = measured_peak()
+        fams = {k: v for k, v in prof.items() if v["launches"]}
+        dom = max(fams, key=lambda k: fams[k]["ms"]) if fams else None
+        roof = None
+        if dom:
+            d = fams[dom]
+            achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9
+            roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+                    "frac": achieved / peak_gbs, "peak_kind": peak_kind,
+                    "traffic": None, "bytes_per_launch": d["bytes"] / d["launches"],
+                    "avg_launch_us": 1e3 * d["ms"] / d["launches"],
+                    "share_of_device_time": d["ms"] / (1e3 * dev_s / world) if dev_s else None}
+        launches = sum(v["launches"] for v in prof.values()) + 2 * args.steps  # + readout kernels
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated circuit)",
+                "config": config_dict(wl, world, {"l2": "flushed between steps (256 MB write)",
+                                                  "peak_live_terms": peak,
+                                                  "term_gate_updates_per_step": updates,
+                                                  "expectation": results[-1]}),
+                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "ms_per_step": 1e3 * e2e_s / args.steps},
+                "gpu_launches": launches,
+                "roofline": roof,
+                "kernel_breakdown": {k: {"ms": round(v["ms"], 3), "launches": v["launches"], "bytes": v["bytes"]}
+                                     for k, v in fams.items()},
+                "clocks": clk.summary(),
+                "wall_s_timed_region": t_wall}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.layers)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,58 @@
+"""Build recipe of the CUDA library (sm_100a), used by __graft_entry__.build().
+
+The library is built in-tree as ppvm_b200/libppvm_cuda.so with nvcc directly: one
+translation unit (csrc/engine.cu) holding the kernels and the C ABI of
+include/ppvm_cuda.h.  -fmad=false keeps every coefficient product and sum a separately
+rounded IEEE operation, as the reference's f64 arithmetic is.
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libppvm_cuda.so")
+SOURCES = [os.path.join(HERE, "csrc", "engine.cu")]
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "kernels.cuh")] + [
+    os.path.join(ROOT, "include", "ppvm_cuda.h")
+]
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
+    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-ffp-contract=off",
+]
+
+
+def nvcc() -> str:
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.exists(cand) else "nvcc"
+
+
+def stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(f) > t for f in SOURCES + HEADERS)
+
+
+def build(force: bool = False, verbose: bool = False, extra=()) -> str:
+    if not force and not stale():
+        return LIB
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", LIB, *SOURCES]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed:\n{r.stdout}\n{r.stderr}")
+    if verbose and r.stderr:
+        print(r.stderr, file=sys.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True,
+          extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else [])

@@ -1,0 +1,1244 @@
+// engine.cu — host side of the C ABI declared in include/ppvm_cuda.h.
+//
+// A ppvm_sum owns SoA term planes on one device plus the scratch the rotation pipeline
+// needs, and one CUDA stream.  Each API call lowers its gates to a list of ops, enqueues
+// the kernels of kernels.cuh for the whole list without host round trips (every kernel
+// reads live counts from the device control block), then synchronises once and checks the
+// device error word.  A rotation that would overflow the term capacity stops before it
+// modifies anything; the call then grows the storage and replays from that op.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ppvm_cuda.h"
+#include "kernels.cuh"
+
+using namespace ppvm;
+
+namespace {
+
+thread_local std::string g_err;
+
+ppvm_status fail(ppvm_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? PPVM_ECAPACITY : PPVM_ECUDA,         \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                   \
+  } while (0)
+
+#define PPVM_TRY(expr)                  \
+  do {                                  \
+    ppvm_status s_ = (expr);            \
+    if (s_ != PPVM_OK) return s_;       \
+  } while (0)
+
+constexpr int kScanBlock = 256;
+constexpr int kPairBlock = 256;
+constexpr int kRedBlock = 256;
+constexpr int kMaxPreserve = 1023;
+const double kHalfPi = 1.5707963267948966;
+
+// host mirror of the device hash (common.cuh) for the preserve-set table
+uint64_t h_mix64(uint64_t v) {
+  v ^= v >> 30;
+  v *= 0xbf58476d1ce4e5b9ull;
+  v ^= v >> 27;
+  v *= 0x94d049bb133111ebull;
+  v ^= v >> 31;
+  return v;
+}
+uint64_t h_hash_key(const uint64_t* x, const uint64_t* z, int W) {
+  uint64_t h = 0x9E3779B97F4A7C15ull;
+  for (int w = 0; w < W; ++w) h = h_mix64(h ^ x[w]) + 0x632BE59BD9B4E019ull;
+  for (int w = 0; w < W; ++w) h = h_mix64(h ^ z[w]) + 0x632BE59BD9B4E019ull;
+  return h;
+}
+
+int g_sm_count = 0;
+
+struct ProfLaunch {
+  int family;
+  int op;
+  int nops;  // ops covered (Clifford runs)
+  cudaEvent_t a, b;
+};
+
+enum Family { F_SCAN = 0, F_PAIR, F_APPLY, F_COMMIT, F_CLIFF, F_TRUNC, F_READ, F_COUNT };
+const char* kFamilyNames[F_COUNT] = {"rot_scan", "rot_pair", "rot_apply", "rot_commit",
+                                     "clifford", "truncate", "readout"};
+
+}  // namespace
+
+struct ppvm_sum {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  uint32_t n = 0;
+  int W = 1;
+  double thr = 1e-10;
+  uint64_t maxw = UINT64_MAX;
+  uint32_t flags = 0;
+  unsigned long long cap = 0;
+  unsigned long long n_host = 0;  // live count at the last synchronisation
+  unsigned long long n_ub = 0;    // upper bound of the live count (sizes grids)
+
+  uint64_t* planes = nullptr;  // x[W*cap] z[W*cap] c[cap]
+  uint32_t* s_idx = nullptr;
+  uint64_t* s_rec = nullptr;
+  uint32_t* partner = nullptr;
+  unsigned long long* table = nullptr;
+  unsigned long long table_cap = 0;
+  unsigned long long* tstate = nullptr;
+  unsigned long long tstate_cap = 0;
+  uint64_t* side = nullptr;
+  Ctrl* d_ctrl = nullptr;
+  Ctrl* h_ctrl = nullptr;
+  OpLog* d_log = nullptr;
+  OpLog* h_log = nullptr;
+  size_t log_cap = 0;
+  size_t last_nops = 0;
+  DevOp* d_ops = nullptr;
+  PatItem* d_pat = nullptr;
+  double* d_partials = nullptr;
+  unsigned long long* d_counter = nullptr;
+  uint64_t* d_pres_keys = nullptr;
+  int* d_pres_table = nullptr;
+  unsigned pres_mask = 0;
+  int npres = 0;
+  std::vector<uint64_t> h_pres;
+
+  unsigned tile_epoch = 0;
+  unsigned table_epoch = 0;
+  bool poisoned = false;
+
+  bool prof = false;
+  std::vector<ProfLaunch> prof_pending;
+  double prof_ms[F_COUNT] = {};
+  uint64_t prof_launches[F_COUNT] = {};
+  uint64_t prof_bytes[F_COUNT] = {};
+
+  Planes planes_view() const {
+    Planes p;
+    p.x = planes;
+    p.z = planes + (size_t)W * cap;
+    p.c = reinterpret_cast<double*>(planes + (size_t)2 * W * cap);
+    p.cap = cap;
+    return p;
+  }
+  unsigned next_tile_epoch() {
+    if (++tile_epoch >= 0xFFFFFu) {
+      cudaMemsetAsync(tstate, 0, tstate_cap * sizeof(unsigned long long), stream);
+      tile_epoch = 1;
+    }
+    return tile_epoch;
+  }
+  unsigned next_table_epoch() {
+    if (++table_epoch >= 0xFFFFu) {
+      cudaMemsetAsync(table, 0, table_cap * sizeof(unsigned long long), stream);
+      table_epoch = 1;
+    }
+    return table_epoch;
+  }
+};
+
+namespace {
+
+unsigned long long next_pow2(unsigned long long v) {
+  unsigned long long p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+ppvm_status ensure_device(int dev) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(PPVM_ENODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= count) return fail(PPVM_EINVAL, "device ordinal out of range");
+  CUDA_TRY(cudaSetDevice(dev));
+  if (g_sm_count == 0) CUDA_TRY(cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev));
+  return PPVM_OK;
+}
+
+void free_scratch(ppvm_sum* s) {
+  cudaFree(s->s_idx);
+  cudaFree(s->s_rec);
+  cudaFree(s->partner);
+  cudaFree(s->table);
+  cudaFree(s->tstate);
+  s->s_idx = nullptr;
+  s->s_rec = nullptr;
+  s->partner = nullptr;
+  s->table = nullptr;
+  s->tstate = nullptr;
+}
+
+// (Re)allocates term storage of capacity new_cap, keeping the first n_host terms.
+ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
+  if (new_cap >= 0xFFFFFFF0ull) return fail(PPVM_ECAPACITY, "term capacity limit (2^32) exceeded");
+  const int W = s->W;
+  uint64_t* np = nullptr;
+  CUDA_TRY(cudaMalloc(&np, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
+  if (s->planes) {
+    for (int w = 0; w < 2 * W + 1; ++w)
+      CUDA_TRY(cudaMemcpyAsync(np + (size_t)w * new_cap, s->planes + (size_t)w * s->cap,
+                               sizeof(uint64_t) * s->n_host, cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    cudaFree(s->planes);
+  }
+  s->planes = np;
+  s->cap = new_cap;
+  free_scratch(s);
+  CUDA_TRY(cudaMalloc(&s->s_idx, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->partner, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->s_rec, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
+  s->table_cap = next_pow2(std::max<unsigned long long>(2 * new_cap, 1024));
+  CUDA_TRY(cudaMalloc(&s->table, sizeof(unsigned long long) * s->table_cap));
+  CUDA_TRY(cudaMemsetAsync(s->table, 0, sizeof(unsigned long long) * s->table_cap, s->stream));
+  s->table_epoch = 0;
+  s->tstate_cap = new_cap / 512 + 64;
+  CUDA_TRY(cudaMalloc(&s->tstate, sizeof(unsigned long long) * s->tstate_cap));
+  CUDA_TRY(cudaMemsetAsync(s->tstate, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
+  s->tile_epoch = 0;
+  return PPVM_OK;
+}
+
+ppvm_status ensure_log(ppvm_sum* s, size_t nops) {
+  if (nops <= s->log_cap) return PPVM_OK;
+  size_t cap = std::max<size_t>(nops, 2 * s->log_cap);
+  cudaFree(s->d_log);
+  cudaFreeHost(s->h_log);
+  s->d_log = nullptr;
+  s->h_log = nullptr;
+  CUDA_TRY(cudaMalloc(&s->d_log, sizeof(OpLog) * cap));
+  CUDA_TRY(cudaMallocHost(&s->h_log, sizeof(OpLog) * cap));
+  s->log_cap = cap;
+  return PPVM_OK;
+}
+
+unsigned grid_for(unsigned long long work, unsigned long long per_block, int max_per_sm) {
+  unsigned long long g = (work + per_block - 1) / per_block;
+  const unsigned long long cap = (unsigned long long)g_sm_count * max_per_sm;
+  if (g > cap) g = cap;
+  if (g == 0) g = 1;
+  return (unsigned)g;
+}
+
+// ---- profiling ------------------------------------------------------------------------------
+struct ProfScope {
+  ppvm_sum* s;
+  ProfLaunch L;
+  bool on;
+  ProfScope(ppvm_sum* sum, int family, int op, int nops) : s(sum), on(sum->prof) {
+    if (!on) return;
+    L.family = family;
+    L.op = op;
+    L.nops = nops;
+    cudaEventCreate(&L.a);
+    cudaEventCreate(&L.b);
+    cudaEventRecord(L.a, s->stream);
+  }
+  ~ProfScope() {
+    if (!on) return;
+    cudaEventRecord(L.b, s->stream);
+    s->prof_pending.push_back(L);
+  }
+};
+
+// Algorithmic bytes of one launch, from the op log ("roofline").
+uint64_t launch_bytes(const ppvm_sum* s, const ProfLaunch& L, const std::vector<int>& test_words) {
+  const uint64_t B = 16ull * s->W + 8;
+  const OpLog& g = s->h_log[L.op];
+  switch (L.family) {
+    case F_SCAN: {
+      const int tw = (L.op < (int)test_words.size()) ? test_words[L.op] : 1;
+      return g.n_in * 8ull * tw + g.n_s * (B + B + 8);  // test words + gather + record/idx/partner
+    }
+    case F_PAIR: return g.n_s * B * 2;                 // own record + partner record
+    case F_APPLY: return g.n_s * (B + 8) + g.n_new * B;  // records, coeff writes, children
+    case F_CLIFF: return 2ull * g.n_in * B;
+    case F_TRUNC: return g.n_in * B + g.n_out * B;
+    default: return 0;
+  }
+}
+
+void prof_collect(ppvm_sum* s, const std::vector<int>& test_words) {
+  for (auto& L : s->prof_pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, L.a, L.b);
+    s->prof_ms[L.family] += ms;
+    s->prof_launches[L.family] += 1;
+    if (L.op >= 0 && (size_t)L.op < s->log_cap) s->prof_bytes[L.family] += launch_bytes(s, L, test_words);
+    cudaEventDestroy(L.a);
+    cudaEventDestroy(L.b);
+  }
+  s->prof_pending.clear();
+}
+
+// ---- op lowering ----------------------------------------------------------------------------
+bool is_clifford_angle(const ppvm_sum* s, double th) {
+  return (s->flags & PPVM_FLAG_CLIFFORD_ANGLES) && (th == kHalfPi || th == -kHalfPi);
+}
+
+// Whether op runs in the fused elementwise pass.
+bool is_local(const ppvm_sum* s, const ppvm_op& op) {
+  switch (op.code) {
+    case PPVM_OP_RX: case PPVM_OP_RY: case PPVM_OP_RZ:
+    case PPVM_OP_RXX: case PPVM_OP_RYY: case PPVM_OP_RZZ:
+      return is_clifford_angle(s, op.theta);
+    case PPVM_OP_TRUNCATE: return false;
+    default: return op.code < PPVM_OP_COUNT_;
+  }
+}
+
+ppvm_status validate(const ppvm_sum* s, const ppvm_op& op) {
+  if (op.code >= PPVM_OP_COUNT_) return fail(PPVM_EINVAL, "unknown op code");
+  if (op.code == PPVM_OP_TRUNCATE) return PPVM_OK;
+  if (op.q0 >= s->n) return fail(PPVM_EINVAL, "qubit index out of range");
+  const bool two = op.code == PPVM_OP_CNOT || op.code == PPVM_OP_CZ || op.code == PPVM_OP_CY ||
+                   op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY || op.code == PPVM_OP_RZZ ||
+                   op.code == PPVM_OP_DEPOLARIZE2;
+  if (two && (op.q1 >= s->n || op.q1 == op.q0))
+    return fail(PPVM_EINVAL, "two-qubit op needs two distinct qubits in range");
+  return PPVM_OK;
+}
+
+DevOp to_devop(const ppvm_op& op) {
+  DevOp d;
+  std::memset(&d, 0, sizeof(d));
+  d.w0 = (uint16_t)(op.q0 >> 6);
+  d.b0 = (uint16_t)(op.q0 & 63);
+  d.w1 = (uint16_t)(op.q1 >> 6);
+  d.b1 = (uint16_t)(op.q1 & 63);
+  switch (op.code) {
+    case PPVM_OP_X: d.code = C_X; break;
+    case PPVM_OP_Y: d.code = C_Y; break;
+    case PPVM_OP_Z: d.code = C_Z; break;
+    case PPVM_OP_H: d.code = C_H; break;
+    case PPVM_OP_S: d.code = C_S; break;
+    case PPVM_OP_S_DAG: d.code = C_SDAG; break;
+    case PPVM_OP_SQRT_X: d.code = C_SQX; break;
+    case PPVM_OP_SQRT_X_DAG: d.code = C_SQXDAG; break;
+    case PPVM_OP_SQRT_Y: d.code = C_SQY; break;
+    case PPVM_OP_SQRT_Y_DAG: d.code = C_SQYDAG; break;
+    case PPVM_OP_CNOT: d.code = C_CNOT; break;
+    case PPVM_OP_CZ: d.code = C_CZ; break;
+    case PPVM_OP_CY: d.code = C_CY; break;
+    case PPVM_OP_PAULI_ERROR: {  // noise.rs:17-37: factors computed as the reference does
+      d.code = C_PAULI_ERROR;
+      const double one = 1.0;
+      d.f0 = one - op.p[1] * 2.0 - op.p[2] * 2.0;  // X
+      d.f1 = one - op.p[0] * 2.0 - op.p[1] * 2.0;  // Z
+      d.f2 = one - op.p[0] * 2.0 - op.p[2] * 2.0;  // Y
+      break;
+    }
+    case PPVM_OP_DEPOLARIZE1: d.code = C_DEP1; d.f0 = 1.0 - op.theta * (4.0 / 3.0); break;
+    case PPVM_OP_DEPOLARIZE2: d.code = C_DEP2; d.f0 = 1.0 - op.theta * (16.0 / 15.0); break;
+    default: {  // Clifford-angle rotation
+      d.code = C_ROTC;
+      const bool gx = op.code == PPVM_OP_RX || op.code == PPVM_OP_RY || op.code == PPVM_OP_RXX ||
+                      op.code == PPVM_OP_RYY;
+      const bool gz = op.code == PPVM_OP_RZ || op.code == PPVM_OP_RY || op.code == PPVM_OP_RZZ ||
+                      op.code == PPVM_OP_RYY;
+      d.two = (op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY || op.code == PPVM_OP_RZZ) ? 1 : 0;
+      d.ax = (uint16_t)((gx ? 1 : 0) | ((gx && d.two) ? 2 : 0));
+      d.az = (uint16_t)((gz ? 1 : 0) | ((gz && d.two) ? 2 : 0));
+      d.f0 = op.theta > 0 ? 1.0 : -1.0;
+      break;
+    }
+  }
+  return d;
+}
+
+void gen_from_op(const ppvm_sum* s, const ppvm_op& op, Gen& g) {
+  std::memset(&g, 0, sizeof(g));
+  auto set = [&](uint32_t q, bool x, bool z) {
+    if (x) g.gx[q >> 6] |= 1ull << (q & 63);
+    if (z) g.gz[q >> 6] |= 1ull << (q & 63);
+  };
+  switch (op.code) {
+    case PPVM_OP_RX: set(op.q0, true, false); break;
+    case PPVM_OP_RY: set(op.q0, true, true); break;
+    case PPVM_OP_RZ: set(op.q0, false, true); break;
+    case PPVM_OP_RXX: set(op.q0, true, false); set(op.q1, true, false); break;
+    case PPVM_OP_RYY: set(op.q0, true, true); set(op.q1, true, true); break;
+    case PPVM_OP_RZZ: set(op.q0, false, true); set(op.q1, false, true); break;
+    default: break;
+  }
+  (void)s;
+}
+
+// ---- kernel enqueue (templated on W) ------------------------------------------------------------
+template <int W>
+struct K {
+  static constexpr int ITEMS = ItemsFor<W>::value;
+  static constexpr unsigned long long TILE = (unsigned long long)kScanBlock * ITEMS;
+
+  static void rotation(ppvm_sum* s, const Gen& g, double theta, int op) {
+    const Planes P = s->planes_view();
+    unsigned xmask = 0, zmask = 0;
+    for (int w = 0; w < W; ++w) {
+      if (g.gz[w]) xmask |= 1u << w;
+      if (g.gx[w]) zmask |= 1u << w;
+    }
+    const double sn = std::sin(theta), cs = std::cos(theta);
+    const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
+    {
+      ProfScope ps(s, F_SCAN, op, 1);
+      k_rot_scan<W, kScanBlock, ITEMS><<<grid_for(nub, TILE, 8), kScanBlock, 0, s->stream>>>(
+          P, s->d_ctrl, g, xmask, zmask, s->s_idx, s->s_rec, s->partner, s->tstate,
+          s->next_tile_epoch(), op, s->d_log);
+    }
+    {
+      ProfScope ps(s, F_PAIR, op, 1);
+      k_rot_pair<W><<<grid_for(nub, kPairBlock, 8), kPairBlock, 0, s->stream>>>(
+          s->d_ctrl, g, s->s_rec, s->partner, s->table, s->table_cap, s->next_table_epoch(), op);
+    }
+    {
+      ProfScope ps(s, F_APPLY, op, 1);
+      k_rot_apply<W, kScanBlock, ITEMS><<<grid_for(nub, TILE, 8), kScanBlock, 0, s->stream>>>(
+          P, s->d_ctrl, g, sn, cs, s->s_idx, s->s_rec, s->partner, s->tstate, s->next_tile_epoch(),
+          op, s->d_log);
+    }
+    {
+      ProfScope ps(s, F_COMMIT, op, 1);
+      k_commit_rot<<<1, 1, 0, s->stream>>>(s->d_ctrl, op, s->d_log);
+    }
+    s->n_ub = std::min<unsigned long long>(s->cap, 2 * s->n_ub);
+  }
+
+  static void clifford(ppvm_sum* s, const DevOp* ops_dev, int nops, int op0) {
+    const Planes P = s->planes_view();
+    ProfScope ps(s, F_CLIFF, op0, nops);
+    k_clifford<W, kCliffBlock><<<grid_for(std::max<unsigned long long>(s->n_ub, 1), kCliffBlock, 16),
+                                 kCliffBlock, 0, s->stream>>>(P, s->d_ctrl, ops_dev, nops, op0, s->d_log);
+  }
+
+  static void truncate(ppvm_sum* s, int op) {
+    const Planes P = s->planes_view();
+    {
+      ProfScope ps(s, F_TRUNC, op, 1);
+      k_truncate<W, kScanBlock, ITEMS><<<grid_for(std::max<unsigned long long>(s->n_ub, 1), TILE, 8),
+                                         kScanBlock, 0, s->stream>>>(
+          P, s->d_ctrl, s->thr, s->maxw, s->d_pres_keys, s->d_pres_table, s->pres_mask, s->npres,
+          s->side, s->tstate, s->next_tile_epoch(), op, s->d_log);
+    }
+    ProfScope ps2(s, F_COMMIT, op, 1);
+    k_commit_truncate<W><<<1, 256, 0, s->stream>>>(P, s->d_ctrl, s->side, op, s->d_log);
+  }
+
+  static void owz(ppvm_sum* s, int nblocks) {
+    k_owz<W><<<nblocks, kRedBlock, 0, s->stream>>>(s->planes_view(), s->d_ctrl, s->d_partials);
+    k_sum_partials<<<1, kRedBlock, 0, s->stream>>>(s->d_partials, nblocks, s->d_ctrl);
+  }
+  static void trace(ppvm_sum* s, int nblocks, int nitems) {
+    k_trace<W><<<nblocks, kRedBlock, 0, s->stream>>>(s->planes_view(), s->d_ctrl, s->d_pat, nitems,
+                                                     s->n, s->d_partials);
+    k_sum_partials<<<1, kRedBlock, 0, s->stream>>>(s->d_partials, nblocks, s->d_ctrl);
+  }
+  static void weights(ppvm_sum* s, uint32_t* out) {
+    k_weights<W><<<grid_for(std::max<unsigned long long>(s->n_host, 1), kRedBlock, 8), kRedBlock, 0,
+                   s->stream>>>(s->planes_view(), s->d_ctrl, out);
+  }
+  static void build_index(ppvm_sum* s, unsigned long long mask, unsigned ep) {
+    k_build_index<W><<<grid_for(std::max<unsigned long long>(s->n_host, 1), kRedBlock, 8), kRedBlock, 0,
+                       s->stream>>>(s->planes_view(), s->d_ctrl, s->table, mask, ep);
+  }
+  static void add_seq(ppvm_sum* s, const uint64_t* nx, const uint64_t* nz, const double* nc,
+                      unsigned long long k, unsigned long long mask, unsigned ep) {
+    k_add_terms_seq<W><<<1, 1, 0, s->stream>>>(s->planes_view(), s->d_ctrl, nx, nz, nc, k, s->table,
+                                                mask, ep);
+  }
+  static void overlap(ppvm_sum* a, ppvm_sum* b, unsigned long long mask, unsigned ep, int nblocks,
+                      unsigned long long* mismatch) {
+    k_overlap<W><<<nblocks, kRedBlock, 0, a->stream>>>(a->planes_view(), b->planes_view(), b->d_ctrl,
+                                                       a->table, mask, ep, a->d_partials, mismatch);
+    k_sum_partials<<<1, kRedBlock, 0, a->stream>>>(a->d_partials, nblocks, a->d_ctrl);
+  }
+};
+
+#define DISPATCH_W(W_, CALL)                 \
+  switch (W_) {                              \
+    case 1: K<1>::CALL; break;               \
+    case 2: K<2>::CALL; break;               \
+    case 3: K<3>::CALL; break;               \
+    case 4: K<4>::CALL; break;               \
+    case 5: K<5>::CALL; break;               \
+    case 6: K<6>::CALL; break;               \
+    case 7: K<7>::CALL; break;               \
+    default: K<8>::CALL; break;              \
+  }
+
+int test_words_of(int W, const Gen& g) {
+  int n = 0;
+  for (int w = 0; w < W; ++w) n += (g.gz[w] != 0) + (g.gx[w] != 0);
+  return n;
+}
+
+// Reads the control block and the op log back; synchronises.
+ppvm_status sync_state(ppvm_sum* s, size_t nops) {
+  CUDA_TRY(cudaMemcpyAsync(s->h_ctrl, s->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s->stream));
+  if (nops) CUDA_TRY(cudaMemcpyAsync(s->h_log, s->d_log, sizeof(OpLog) * nops, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return PPVM_OK;
+}
+
+ppvm_status clear_err(ppvm_sum* s) {
+  Ctrl c = *s->h_ctrl;
+  c.err = 0;
+  c.err_op = 0;
+  for (int t = 0; t < 4; ++t) c.tickets[t] = 0;
+  CUDA_TRY(cudaMemcpyAsync(s->d_ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return PPVM_OK;
+}
+
+// Enqueues ops[start..n) (gate-list indices start..n).  Generators of explicit Pauli rotations
+// come from `gens` when ops[i].flags == 1 (index in q0).
+ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
+                    const std::vector<Gen>& gens, std::vector<int>& test_words) {
+  std::vector<DevOp> run;
+  int run_start = -1;
+  auto flush = [&]() -> ppvm_status {
+    size_t off = 0;
+    while (off < run.size()) {
+      const int cnt = (int)std::min<size_t>(kMaxOpsPerLaunch, run.size() - off);
+      CUDA_TRY(cudaMemcpyAsync(s->d_ops, run.data() + off, sizeof(DevOp) * cnt,
+                               cudaMemcpyHostToDevice, s->stream));
+      DISPATCH_W(s->W, clifford(s, s->d_ops, cnt, run_start + (int)off));
+      off += cnt;
+    }
+    run.clear();
+    run_start = -1;
+    return PPVM_OK;
+  };
+  for (size_t i = start; i < n_ops; ++i) {
+    const ppvm_op& op = ops[i];
+    if (op.flags == 1) {  // explicit generator
+      PPVM_TRY(flush());
+      const Gen& g = gens[op.q0];
+      test_words[i] = test_words_of(s->W, g);
+      bool cliff = is_clifford_angle(s, op.theta);
+      if (cliff) {
+        return fail(PPVM_EINVAL, "internal: explicit Clifford-angle generators are lowered earlier");
+      }
+      DISPATCH_W(s->W, rotation(s, g, op.theta, (int)i));
+      continue;
+    }
+    if (op.code == PPVM_OP_TRUNCATE) {
+      PPVM_TRY(flush());
+      DISPATCH_W(s->W, truncate(s, (int)i));
+      continue;
+    }
+    if (is_local(s, op)) {
+      if (run.empty()) run_start = (int)i;
+      run.push_back(to_devop(op));
+      continue;
+    }
+    PPVM_TRY(flush());
+    Gen g;
+    gen_from_op(s, op, g);
+    test_words[i] = test_words_of(s->W, g);
+    DISPATCH_W(s->W, rotation(s, g, op.theta, (int)i));
+  }
+  PPVM_TRY(flush());
+  CUDA_TRY(cudaGetLastError());
+  return PPVM_OK;
+}
+
+// Runs a validated op list with capacity growth and replay.
+ppvm_status run_list(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, const std::vector<Gen>& gens) {
+  if (s->poisoned) return fail(PPVM_ECUDA, "sum is in an error state from an earlier failure");
+  PPVM_TRY(ensure_device(s->device));
+  PPVM_TRY(ensure_log(s, std::max<size_t>(n_ops, 1)));
+  std::vector<int> test_words(n_ops, 0);
+  size_t start = 0;
+  for (int attempt = 0; attempt < 64; ++attempt) {
+    PPVM_TRY(enqueue(s, ops, n_ops, start, gens, test_words));
+    PPVM_TRY(sync_state(s, n_ops));
+    const Ctrl& c = *s->h_ctrl;
+    s->n_host = c.n;
+    if (c.err == kOk) {
+      s->n_ub = s->n_host;
+      s->last_nops = n_ops;
+      if (s->prof) prof_collect(s, test_words);
+      return PPVM_OK;
+    }
+    if (s->prof) prof_collect(s, test_words);
+    if (c.err == kErrCapacity && c.err_op >= 0 && (size_t)c.err_op >= start) {
+      const unsigned long long need = c.cap_needed;
+      start = (size_t)c.err_op;
+      PPVM_TRY(clear_err(s));
+      unsigned long long nc = std::max<unsigned long long>(2 * s->cap, need + need / 2 + 1024);
+      if (nc >= 0xFFFFFFF0ull) nc = std::max<unsigned long long>(need, 0xFFFFFFF0ull - 1);
+      ppvm_status st = grow(s, nc);
+      if (st != PPVM_OK) {
+        s->poisoned = true;
+        return st;
+      }
+      s->n_ub = s->n_host;
+      continue;
+    }
+    s->poisoned = true;
+    if (c.err == kErrTimeout) return fail(PPVM_ETIMEOUT, "device wait timed out (op " + std::to_string(c.err_op) + ")");
+    return fail(PPVM_ECUDA, "device error " + std::to_string(c.err) + " at op " + std::to_string(c.err_op));
+  }
+  s->poisoned = true;
+  return fail(PPVM_ECAPACITY, "capacity growth did not converge");
+}
+
+ppvm_status run_gate(ppvm_sum* s, uint32_t code, const uint32_t* t, size_t k, bool pairs, double theta,
+                     const double* p, int truncate) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  if (k && !t) return fail(PPVM_EINVAL, "null target list");
+  if (pairs && (k % 2)) return fail(PPVM_EINVAL, "two-qubit operations require an even number of targets");
+  std::vector<ppvm_op> ops;
+  const size_t step = pairs ? 2 : 1;
+  for (size_t i = 0; i < k; i += step) {
+    ppvm_op op;
+    std::memset(&op, 0, sizeof(op));
+    op.code = code;
+    op.q0 = t[i];
+    op.q1 = pairs ? t[i + 1] : 0;
+    op.theta = theta;
+    if (p) for (int j = 0; j < 3; ++j) op.p[j] = p[j];
+    PPVM_TRY(validate(s, op));
+    ops.push_back(op);
+  }
+  if (truncate) {
+    ppvm_op op;
+    std::memset(&op, 0, sizeof(op));
+    op.code = PPVM_OP_TRUNCATE;
+    ops.push_back(op);
+  }
+  if (ops.empty()) return PPVM_OK;
+  return run_list(s, ops.data(), ops.size(), {});
+}
+
+ppvm_status do_reduce_owz(ppvm_sum* s, double* out) {
+  const int nb = (int)grid_for(std::max<unsigned long long>(s->n_host, 1), kRedBlock * 4, 2);
+  DISPATCH_W(s->W, owz(s, nb));
+  CUDA_TRY(cudaGetLastError());
+  PPVM_TRY(sync_state(s, 0));
+  *out = s->h_ctrl->sum;
+  return PPVM_OK;
+}
+
+// PauliPattern grammar (crates/ppvm-pauli-word/src/pattern/parse.rs:32-127) -> PatItems.
+// Accept bits: 1 = I, 2 = X, 4 = Z, 8 = Y; '_' accepts only I, as the reference matcher does.
+bool parse_pattern(const char* text, std::vector<PatItem>& out) {
+  std::string in(text);
+  size_t b = in.find_first_not_of(" \t\n\r"), e = in.find_last_not_of(" \t\n\r");
+  in = (b == std::string::npos) ? std::string() : in.substr(b, e - b + 1);
+  auto bit = [](char c) -> unsigned { return c == 'X' ? 2u : c == 'Z' ? 4u : c == 'Y' ? 8u : 0u; };
+  size_t i = 0;
+  while (i < in.size()) {
+    const char c = in[i++];
+    unsigned acc;
+    if (c == '[') {
+      unsigned set = 0;
+      while (i < in.size()) {  // an unclosed '[' ends at the end of the text, as in parse.rs
+        const char d = in[i];
+        if (d == ']') {
+          ++i;
+          break;
+        }
+        if (!bit(d)) return false;
+        set |= bit(d);
+        ++i;
+      }
+      if (!set) return false;
+      acc = set;
+    } else if (c == '_') {
+      acc = 1u;
+    } else if (bit(c)) {
+      acc = bit(c);
+    } else {
+      return false;
+    }
+    if (i < in.size() && in[i] == '?') {
+      ++i;
+      acc |= 1u;
+    }
+    PatItem it;
+    it.accept = acc;
+    it.arg = 0;
+    if (i < in.size() && in[i] == '*') {
+      ++i;
+      it.kind = 1;
+    } else if (i < in.size() && in[i] == '{') {
+      ++i;
+      std::string num;
+      while (i < in.size() && isdigit((unsigned char)in[i])) num.push_back(in[i++]);
+      if (i >= in.size() || in[i] != '}' || num.empty()) return false;
+      ++i;
+      it.kind = 2;
+      it.arg = std::stoull(num);
+    } else if (i < in.size() && isdigit((unsigned char)in[i])) {
+      std::string num;
+      while (i < in.size() && isdigit((unsigned char)in[i])) num.push_back(in[i++]);
+      it.kind = 0;
+      it.arg = std::stoull(num);
+    } else {
+      return false;
+    }
+    out.push_back(it);
+  }
+  return true;
+}
+
+// Builds the sum's key index (table slot -> term) for the cold lookup paths.
+ppvm_status build_index(ppvm_sum* s, unsigned long long expected, unsigned long long* mask_out,
+                        unsigned* epoch_out) {
+  unsigned long long tsize = next_pow2(std::max<unsigned long long>(2 * expected, 1024));
+  if (tsize > s->table_cap) return fail(PPVM_ECAPACITY, "index table too small");
+  const unsigned ep = s->next_table_epoch();
+  DISPATCH_W(s->W, build_index(s, tsize - 1, ep));
+  *mask_out = tsize - 1;
+  *epoch_out = ep;
+  return PPVM_OK;
+}
+
+}  // namespace
+
+// =============================================================================================
+extern "C" {
+
+const char* ppvm_last_error_string(void) { return g_err.c_str(); }
+const char* ppvm_version(void) { return "ppvm_b200 0.1 (sm_100a)"; }
+
+ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_coeff, uint64_t max_weight,
+                             size_t capacity_hint, uint32_t flags, int device) {
+  if (!out) return fail(PPVM_EINVAL, "null out pointer");
+  *out = nullptr;
+  if (n_qubits == 0 || n_qubits > 64 * kMaxW)
+    return fail(PPVM_EINVAL, "n_qubits must be in [1, 512]");
+  PPVM_TRY(ensure_device(device));
+  ppvm_sum* s = new ppvm_sum();
+  s->device = device;
+  s->n = n_qubits;
+  s->W = (int)((n_qubits + 63) / 64);
+  s->thr = min_abs_coeff;
+  s->maxw = max_weight;
+  s->flags = flags;
+  auto bail = [&](ppvm_status st) {
+    ppvm_sum_destroy(s);
+    return st;
+  };
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(PPVM_ECUDA, "cudaStreamCreate failed"));
+  if (cudaMalloc(&s->d_ctrl, sizeof(Ctrl)) != cudaSuccess ||
+      cudaMallocHost(&s->h_ctrl, sizeof(Ctrl)) != cudaSuccess ||
+      cudaMalloc(&s->d_ops, sizeof(DevOp) * kMaxOpsPerLaunch) != cudaSuccess ||
+      cudaMalloc(&s->d_partials, sizeof(double) * 8192) != cudaSuccess ||
+      cudaMalloc(&s->d_counter, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&s->side, sizeof(uint64_t) * (2 * s->W + 1) * (kMaxPreserve + 1)) != cudaSuccess)
+    return bail(fail(PPVM_ECAPACITY, "device allocation failed"));
+  std::memset(s->h_ctrl, 0, sizeof(Ctrl));
+  if (cudaMemsetAsync(s->d_ctrl, 0, sizeof(Ctrl), s->stream) != cudaSuccess)
+    return bail(fail(PPVM_ECUDA, "memset failed"));
+  ppvm_status st = grow(s, std::max<size_t>(capacity_hint, 4096));
+  if (st != PPVM_OK) return bail(st);
+  st = ensure_log(s, 64);
+  if (st != PPVM_OK) return bail(st);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return bail(fail(PPVM_ECUDA, "sync failed"));
+  *out = s;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_sum_create(ppvm_sum** out, uint32_t n_qubits, double min_abs_coeff, uint64_t max_weight,
+                            size_t capacity_hint) {
+  return ppvm_sum_create2(out, n_qubits, min_abs_coeff, max_weight, capacity_hint, 0, 0);
+}
+
+ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
+  if (!s) return PPVM_OK;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto& L : s->prof_pending) {
+    cudaEventDestroy(L.a);
+    cudaEventDestroy(L.b);
+  }
+  cudaFree(s->planes);
+  free_scratch(s);
+  cudaFree(s->side);
+  cudaFree(s->d_ctrl);
+  cudaFreeHost(s->h_ctrl);
+  cudaFree(s->d_log);
+  cudaFreeHost(s->h_log);
+  cudaFree(s->d_ops);
+  cudaFree(s->d_pat);
+  cudaFree(s->d_partials);
+  cudaFree(s->d_counter);
+  cudaFree(s->d_pres_keys);
+  cudaFree(s->d_pres_table);
+  if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_sum_set_stream(ppvm_sum* s, void* cuda_stream) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  if (s->own_stream) cudaStreamDestroy(s->stream);
+  if (cuda_stream) {
+    s->stream = (cudaStream_t)cuda_stream;
+    s->own_stream = false;
+  } else {
+    CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->own_stream = true;
+  }
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_sum_clone(const ppvm_sum* src, ppvm_sum** out) {
+  if (!src || !out) return fail(PPVM_EINVAL, "null argument");
+  ppvm_sum* d = nullptr;
+  PPVM_TRY(ppvm_sum_create2(&d, src->n, src->thr, src->maxw, std::max<unsigned long long>(src->cap, 4096),
+                            src->flags, src->device));
+  ppvm_sum* s = const_cast<ppvm_sum*>(src);
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  for (int w = 0; w < 2 * src->W + 1; ++w)
+    CUDA_TRY(cudaMemcpyAsync(d->planes + (size_t)w * d->cap, src->planes + (size_t)w * src->cap,
+                             sizeof(uint64_t) * src->n_host, cudaMemcpyDeviceToDevice, d->stream));
+  d->n_host = src->n_host;
+  d->n_ub = src->n_host;
+  Ctrl c;
+  std::memset(&c, 0, sizeof(c));
+  c.n = src->n_host;
+  CUDA_TRY(cudaMemcpyAsync(d->d_ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, d->stream));
+  if (src->npres) {
+    std::vector<uint64_t> x, z;
+    for (int j = 0; j < src->npres; ++j)
+      for (int w = 0; w < src->W; ++w) {
+        x.push_back(src->h_pres[(size_t)j * 2 * src->W + w]);
+        z.push_back(src->h_pres[(size_t)j * 2 * src->W + src->W + w]);
+      }
+    PPVM_TRY(ppvm_sum_set_preserve(d, x.data(), z.data(), src->npres));
+  }
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  *out = d;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_len(const ppvm_sum* s, size_t* out) {
+  if (!s || !out) return fail(PPVM_EINVAL, "null argument");
+  *out = (size_t)s->n_host;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_sum_add_terms(ppvm_sum* s, const uint64_t* x, const uint64_t* z, const double* c, size_t k) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  if (k == 0) return PPVM_OK;
+  if (!x || !z || !c) return fail(PPVM_EINVAL, "null term arrays");
+  if (s->poisoned) return fail(PPVM_ECUDA, "sum is in an error state from an earlier failure");
+  const int W = s->W;
+  // bits beyond n must be clear
+  const int tail = (int)(s->n % 64);
+  for (size_t i = 0; i < k; ++i) {
+    if (tail && ((x[i * W + W - 1] | z[i * W + W - 1]) >> tail))
+      return fail(PPVM_EINVAL, "word has bits set at or above n_qubits");
+  }
+  PPVM_TRY(ensure_device(s->device));
+  if (s->n_host + k > s->cap) PPVM_TRY(grow(s, std::max<unsigned long long>(2 * s->cap, s->n_host + k + 1024)));
+  uint64_t* dx = nullptr;
+  CUDA_TRY(cudaMalloc(&dx, sizeof(uint64_t) * (2 * W + 1) * k));
+  uint64_t* dz = dx + W * k;
+  double* dc = reinterpret_cast<double*>(dx + 2 * W * k);
+  CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(uint64_t) * W * k, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(cudaMemcpyAsync(dz, z, sizeof(uint64_t) * W * k, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(cudaMemcpyAsync(dc, c, sizeof(double) * k, cudaMemcpyHostToDevice, s->stream));
+  unsigned long long mask;
+  unsigned ep;
+  ppvm_status st = build_index(s, s->n_host + k, &mask, &ep);
+  if (st == PPVM_OK) {
+    DISPATCH_W(W, add_seq(s, dx, dz, dc, k, mask, ep));
+    st = sync_state(s, 0);
+  }
+  cudaFree(dx);
+  PPVM_TRY(st);
+  if (s->h_ctrl->err) {
+    s->poisoned = true;
+    return fail(PPVM_ECUDA, "device error while adding terms");
+  }
+  s->n_host = s->h_ctrl->n;
+  s->n_ub = s->n_host;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_sum_add_string(ppvm_sum* s, const char* word, double c) {
+  if (!s || !word) return fail(PPVM_EINVAL, "null argument");
+  std::vector<uint64_t> x(s->W, 0), z(s->W, 0);
+  uint32_t q = 0;
+  for (const char* p = word; *p; ++p) {
+    const char ch = *p;
+    if (ch == '_') continue;
+    if (q >= s->n) return fail(PPVM_EINVAL, "word longer than n_qubits");
+    const uint64_t b = 1ull << (q & 63);
+    if (ch == 'X') x[q >> 6] |= b;
+    else if (ch == 'Z') z[q >> 6] |= b;
+    else if (ch == 'Y') { x[q >> 6] |= b; z[q >> 6] |= b; }
+    else if (ch != 'I') return fail(PPVM_EINVAL, std::string("Invalid Pauli character: ") + ch);
+    ++q;
+  }
+  if (q != s->n) return fail(PPVM_EINVAL, "word length differs from n_qubits");
+  return ppvm_sum_add_terms(s, x.data(), z.data(), &c, 1);
+}
+
+ppvm_status ppvm_sum_set_preserve(ppvm_sum* s, const uint64_t* x, const uint64_t* z, size_t k) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  if (k > (size_t)kMaxPreserve) return fail(PPVM_EINVAL, "at most 1023 preserve strings are supported");
+  if (k && (!x || !z)) return fail(PPVM_EINVAL, "null preserve arrays");
+  PPVM_TRY(ensure_device(s->device));
+  const int W = s->W;
+  cudaFree(s->d_pres_keys);
+  cudaFree(s->d_pres_table);
+  s->d_pres_keys = nullptr;
+  s->d_pres_table = nullptr;
+  s->npres = 0;
+  s->h_pres.clear();
+  if (k == 0) return PPVM_OK;
+  // de-duplicate (a HashSet in the reference builder, data.rs:75-77)
+  std::vector<uint64_t> keys;
+  for (size_t i = 0; i < k; ++i) {
+    bool dup = false;
+    for (size_t j = 0; j < keys.size() / (2 * W) && !dup; ++j) {
+      bool eq = true;
+      for (int w = 0; w < W; ++w) eq &= keys[j * 2 * W + w] == x[i * W + w] && keys[j * 2 * W + W + w] == z[i * W + w];
+      dup = eq;
+    }
+    if (dup) continue;
+    for (int w = 0; w < W; ++w) keys.push_back(x[i * W + w]);
+    for (int w = 0; w < W; ++w) keys.push_back(z[i * W + w]);
+  }
+  const int np = (int)(keys.size() / (2 * W));
+  const unsigned tsize = 2048;
+  std::vector<int> table(tsize, -1);
+  for (int j = 0; j < np; ++j) {
+    unsigned slot = (unsigned)(h_hash_key(&keys[(size_t)j * 2 * W], &keys[(size_t)j * 2 * W + W], W) & (tsize - 1));
+    while (table[slot] >= 0) slot = (slot + 1) & (tsize - 1);
+    table[slot] = j;
+  }
+  CUDA_TRY(cudaMalloc(&s->d_pres_keys, sizeof(uint64_t) * keys.size()));
+  CUDA_TRY(cudaMalloc(&s->d_pres_table, sizeof(int) * tsize));
+  CUDA_TRY(cudaMemcpyAsync(s->d_pres_keys, keys.data(), sizeof(uint64_t) * keys.size(), cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(cudaMemcpyAsync(s->d_pres_table, table.data(), sizeof(int) * tsize, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  s->pres_mask = tsize - 1;
+  s->npres = np;
+  s->h_pres = keys;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_export_terms(const ppvm_sum* cs, uint64_t* x, uint64_t* z, double* c, size_t cap, size_t* n_out) {
+  if (!cs || !n_out) return fail(PPVM_EINVAL, "null argument");
+  ppvm_sum* s = const_cast<ppvm_sum*>(cs);
+  PPVM_TRY(ensure_device(s->device));
+  const size_t n = std::min<size_t>(cap, s->n_host);
+  *n_out = n;
+  if (n == 0) return PPVM_OK;
+  if (!x || !z || !c) return fail(PPVM_EINVAL, "null output arrays");
+  const int W = s->W;
+  std::vector<uint64_t> buf((size_t)(2 * W) * n);
+  for (int w = 0; w < 2 * W; ++w)
+    CUDA_TRY(cudaMemcpyAsync(buf.data() + (size_t)w * n, s->planes + (size_t)w * s->cap, sizeof(uint64_t) * n,
+                             cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(cudaMemcpyAsync(c, s->planes + (size_t)2 * W * s->cap, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                           s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  for (size_t i = 0; i < n; ++i)
+    for (int w = 0; w < W; ++w) {
+      x[i * W + w] = buf[(size_t)w * n + i];
+      z[i * W + w] = buf[(size_t)(W + w) * n + i];
+    }
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_weights(const ppvm_sum* cs, uint32_t* w, size_t cap, size_t* n_out) {
+  if (!cs || !n_out) return fail(PPVM_EINVAL, "null argument");
+  ppvm_sum* s = const_cast<ppvm_sum*>(cs);
+  PPVM_TRY(ensure_device(s->device));
+  const size_t n = std::min<size_t>(cap, s->n_host);
+  *n_out = n;
+  if (n == 0) return PPVM_OK;
+  if (!w) return fail(PPVM_EINVAL, "null output array");
+  uint32_t* d = reinterpret_cast<uint32_t*>(s->s_idx);  // scratch, cap entries
+  DISPATCH_W(s->W, weights(s, d));
+  CUDA_TRY(cudaMemcpyAsync(w, d, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_current_max_weight(const ppvm_sum* s, uint64_t* out) {
+  if (!s || !out) return fail(PPVM_EINVAL, "null argument");
+  std::vector<uint32_t> w(s->n_host);
+  size_t n = 0;
+  PPVM_TRY(ppvm_weights(s, w.data(), w.size(), &n));
+  uint64_t m = 0;
+  for (size_t i = 0; i < n; ++i) m = std::max<uint64_t>(m, w[i]);
+  *out = m;
+  return PPVM_OK;
+}
+
+#define GATE1(name, CODE)                                                                     \
+  ppvm_status name(ppvm_sum* s, const uint32_t* t, size_t k, int truncate) {                  \
+    return run_gate(s, CODE, t, k, false, 0.0, nullptr, truncate);                            \
+  }
+#define GATE2(name, CODE)                                                                     \
+  ppvm_status name(ppvm_sum* s, const uint32_t* t, size_t k, int truncate) {                  \
+    return run_gate(s, CODE, t, k, true, 0.0, nullptr, truncate);                             \
+  }
+#define ROT1(name, CODE)                                                                      \
+  ppvm_status name(ppvm_sum* s, const uint32_t* t, size_t k, double theta, int truncate) {    \
+    return run_gate(s, CODE, t, k, false, theta, nullptr, truncate);                          \
+  }
+#define ROT2(name, CODE)                                                                      \
+  ppvm_status name(ppvm_sum* s, const uint32_t* t, size_t k, double theta, int truncate) {    \
+    return run_gate(s, CODE, t, k, true, theta, nullptr, truncate);                           \
+  }
+
+GATE1(ppvm_x, PPVM_OP_X)
+GATE1(ppvm_y, PPVM_OP_Y)
+GATE1(ppvm_z, PPVM_OP_Z)
+GATE1(ppvm_h, PPVM_OP_H)
+GATE1(ppvm_s, PPVM_OP_S)
+GATE1(ppvm_s_dag, PPVM_OP_S_DAG)
+GATE1(ppvm_sqrt_x, PPVM_OP_SQRT_X)
+GATE1(ppvm_sqrt_x_dag, PPVM_OP_SQRT_X_DAG)
+GATE1(ppvm_sqrt_y, PPVM_OP_SQRT_Y)
+GATE1(ppvm_sqrt_y_dag, PPVM_OP_SQRT_Y_DAG)
+GATE2(ppvm_cnot, PPVM_OP_CNOT)
+GATE2(ppvm_cz, PPVM_OP_CZ)
+GATE2(ppvm_cy, PPVM_OP_CY)
+ROT1(ppvm_rx, PPVM_OP_RX)
+ROT1(ppvm_ry, PPVM_OP_RY)
+ROT1(ppvm_rz, PPVM_OP_RZ)
+ROT2(ppvm_rxx, PPVM_OP_RXX)
+ROT2(ppvm_ryy, PPVM_OP_RYY)
+ROT2(ppvm_rzz, PPVM_OP_RZZ)
+
+ppvm_status ppvm_r(ppvm_sum* s, uint32_t q, double axis_angle, double theta, int truncate) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  ppvm_op ops[4];
+  std::memset(ops, 0, sizeof(ops));
+  ops[0].code = PPVM_OP_RZ; ops[0].q0 = q; ops[0].theta = axis_angle;
+  ops[1].code = PPVM_OP_RX; ops[1].q0 = q; ops[1].theta = theta;
+  ops[2].code = PPVM_OP_RZ; ops[2].q0 = q; ops[2].theta = -axis_angle;
+  ops[3].code = PPVM_OP_TRUNCATE;
+  for (int i = 0; i < 3; ++i) PPVM_TRY(validate(s, ops[i]));
+  return run_list(s, ops, truncate ? 4 : 3, {});
+}
+
+ppvm_status ppvm_pauli_error(ppvm_sum* s, const uint32_t* t, size_t k, const double p[3], int truncate) {
+  if (!p) return fail(PPVM_EINVAL, "null probabilities");
+  return run_gate(s, PPVM_OP_PAULI_ERROR, t, k, false, 0.0, p, truncate);
+}
+ppvm_status ppvm_depolarize1(ppvm_sum* s, const uint32_t* t, size_t k, double p, int truncate) {
+  return run_gate(s, PPVM_OP_DEPOLARIZE1, t, k, false, p, nullptr, truncate);
+}
+ppvm_status ppvm_depolarize2(ppvm_sum* s, const uint32_t* t, size_t k, double p, int truncate) {
+  return run_gate(s, PPVM_OP_DEPOLARIZE2, t, k, true, p, nullptr, truncate);
+}
+
+ppvm_status ppvm_pauli_rotation(ppvm_sum* s, const uint64_t* gx, const uint64_t* gz, double theta, int truncate) {
+  if (!s || !gx || !gz) return fail(PPVM_EINVAL, "null argument");
+  const int W = s->W;
+  const int tail = (int)(s->n % 64);
+  if (tail && ((gx[W - 1] | gz[W - 1]) >> tail)) return fail(PPVM_EINVAL, "generator has bits at or above n_qubits");
+  bool any = false;
+  for (int w = 0; w < W; ++w) any |= (gx[w] | gz[w]) != 0;
+  std::vector<Gen> gens(1);
+  std::memset(&gens[0], 0, sizeof(Gen));
+  for (int w = 0; w < W; ++w) {
+    gens[0].gx[w] = gx[w];
+    gens[0].gz[w] = gz[w];
+  }
+  std::vector<ppvm_op> ops;
+  if (any) {
+    if (is_clifford_angle(s, theta)) {
+      // Clifford-angle generic rotation: run it through the rotation pipeline with cos = 0
+      // is not equivalent (the parent would remain with coefficient 0); lower to ops when the
+      // support is 1-2 qubits, else reject.
+      std::vector<uint32_t> sup;
+      for (uint32_t q = 0; q < s->n; ++q)
+        if (((gx[q >> 6] | gz[q >> 6]) >> (q & 63)) & 1) sup.push_back(q);
+      if (sup.size() > 2) return fail(PPVM_EINVAL, "Clifford-angle mode supports generic rotations on <= 2 qubits");
+      auto axis = [&](uint32_t q) { return (int)((gx[q >> 6] >> (q & 63)) & 1) | ((int)((gz[q >> 6] >> (q & 63)) & 1) << 1); };
+      ppvm_op op;
+      std::memset(&op, 0, sizeof(op));
+      op.theta = theta;
+      op.q0 = sup[0];
+      if (sup.size() == 1) {
+        const int a = axis(sup[0]);
+        op.code = a == 1 ? PPVM_OP_RX : a == 2 ? PPVM_OP_RZ : PPVM_OP_RY;
+      } else {
+        const int a = axis(sup[0]), b = axis(sup[1]);
+        if (a != b) return fail(PPVM_EINVAL, "Clifford-angle mode supports XX, YY, ZZ two-qubit generators");
+        op.q1 = sup[1];
+        op.code = a == 1 ? PPVM_OP_RXX : a == 2 ? PPVM_OP_RZZ : PPVM_OP_RYY;
+      }
+      ops.push_back(op);
+    } else {
+      ppvm_op op;
+      std::memset(&op, 0, sizeof(op));
+      op.code = PPVM_OP_RX;  // placeholder code; flags = 1 selects gens[q0]
+      op.flags = 1;
+      op.q0 = 0;
+      op.theta = theta;
+      ops.push_back(op);
+    }
+  }
+  if (truncate) {
+    ppvm_op op;
+    std::memset(&op, 0, sizeof(op));
+    op.code = PPVM_OP_TRUNCATE;
+    ops.push_back(op);
+  }
+  if (ops.empty()) return PPVM_OK;
+  return run_list(s, ops.data(), ops.size(), gens);
+}
+
+ppvm_status ppvm_truncate(ppvm_sum* s) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  ppvm_op op;
+  std::memset(&op, 0, sizeof(op));
+  op.code = PPVM_OP_TRUNCATE;
+  return run_list(s, &op, 1, {});
+}
+
+ppvm_status ppvm_gate_list_run(ppvm_sum* s, const ppvm_op* ops, size_t n_ops) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  if (n_ops && !ops) return fail(PPVM_EINVAL, "null op list");
+  for (size_t i = 0; i < n_ops; ++i) {
+    if (ops[i].flags != 0) return fail(PPVM_EINVAL, "op flags must be 0");
+    PPVM_TRY(validate(s, ops[i]));
+  }
+  if (n_ops == 0) return PPVM_OK;
+  return run_list(s, ops, n_ops, {});
+}
+
+ppvm_status ppvm_last_run_live_counts(const ppvm_sum* s, uint64_t* counts, size_t cap, size_t* n_out) {
+  if (!s || !n_out) return fail(PPVM_EINVAL, "null argument");
+  *n_out = s->last_nops;
+  const size_t n = std::min(cap, s->last_nops);
+  if (n && !counts) return fail(PPVM_EINVAL, "null output");
+  for (size_t i = 0; i < n; ++i) counts[i] = s->h_log[i].n_in;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_overlap_with_zero(ppvm_sum* s, double* out) {
+  if (!s || !out) return fail(PPVM_EINVAL, "null argument");
+  PPVM_TRY(ensure_device(s->device));
+  return do_reduce_owz(s, out);
+}
+
+ppvm_status ppvm_expectation(ppvm_sum* s, double* out) { return ppvm_overlap_with_zero(s, out); }
+
+ppvm_status ppvm_trace(ppvm_sum* s, const char* pattern, double* out) {
+  if (!s || !pattern || !out) return fail(PPVM_EINVAL, "null argument");
+  std::vector<PatItem> items;
+  if (!parse_pattern(pattern, items)) return fail(PPVM_EINVAL, std::string("bad Pauli pattern: ") + pattern);
+  PPVM_TRY(ensure_device(s->device));
+  if (items.size() == 1 && items[0].kind == 1 && items[0].accept == (1u | 4u))  // "Z?*"
+    return do_reduce_owz(s, out);
+  cudaFree(s->d_pat);
+  s->d_pat = nullptr;
+  CUDA_TRY(cudaMalloc(&s->d_pat, sizeof(PatItem) * std::max<size_t>(items.size(), 1)));
+  if (!items.empty())
+    CUDA_TRY(cudaMemcpyAsync(s->d_pat, items.data(), sizeof(PatItem) * items.size(), cudaMemcpyHostToDevice, s->stream));
+  const int nb = (int)grid_for(std::max<unsigned long long>(s->n_host, 1), kRedBlock * 4, 2);
+  DISPATCH_W(s->W, trace(s, nb, (int)items.size()));
+  CUDA_TRY(cudaGetLastError());
+  PPVM_TRY(sync_state(s, 0));
+  *out = s->h_ctrl->sum;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_overlap(ppvm_sum* a, ppvm_sum* b, double* out) {
+  if (!a || !b || !out) return fail(PPVM_EINVAL, "null argument");
+  if (a->n != b->n) return fail(PPVM_EINVAL, "sums have different qubit counts");
+  if (a->device != b->device) return fail(PPVM_EINVAL, "sums live on different devices");
+  PPVM_TRY(ensure_device(a->device));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  unsigned long long mask;
+  unsigned ep;
+  PPVM_TRY(build_index(a, a->n_host, &mask, &ep));
+  CUDA_TRY(cudaMemsetAsync(a->d_counter, 0, sizeof(unsigned long long), a->stream));
+  const int nb = (int)grid_for(std::max<unsigned long long>(b->n_host, 1), kRedBlock * 4, 2);
+  DISPATCH_W(a->W, overlap(a, b, mask, ep, nb, a->d_counter));
+  CUDA_TRY(cudaGetLastError());
+  PPVM_TRY(sync_state(a, 0));
+  *out = a->h_ctrl->sum;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_equal(const ppvm_sum* ca, const ppvm_sum* cb, int* out) {
+  if (!ca || !cb || !out) return fail(PPVM_EINVAL, "null argument");
+  ppvm_sum* a = const_cast<ppvm_sum*>(ca);
+  ppvm_sum* b = const_cast<ppvm_sum*>(cb);
+  *out = 0;
+  if (a->n != b->n || a->n_host != b->n_host) return PPVM_OK;
+  if (a->n_host == 0) {
+    *out = 1;
+    return PPVM_OK;
+  }
+  PPVM_TRY(ensure_device(a->device));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  unsigned long long mask;
+  unsigned ep;
+  PPVM_TRY(build_index(a, a->n_host, &mask, &ep));
+  CUDA_TRY(cudaMemsetAsync(a->d_counter, 0, sizeof(unsigned long long), a->stream));
+  const int nb = (int)grid_for(std::max<unsigned long long>(b->n_host, 1), kRedBlock * 4, 2);
+  DISPATCH_W(a->W, overlap(a, b, mask, ep, nb, a->d_counter));
+  unsigned long long miss = 1;
+  CUDA_TRY(cudaMemcpyAsync(&miss, a->d_counter, sizeof(miss), cudaMemcpyDeviceToHost, a->stream));
+  CUDA_TRY(cudaStreamSynchronize(a->stream));
+  *out = miss == 0 ? 1 : 0;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_profile_enable(ppvm_sum* s, int on) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  s->prof = on != 0;
+  if (on) {
+    for (int f = 0; f < F_COUNT; ++f) {
+      s->prof_ms[f] = 0;
+      s->prof_launches[f] = 0;
+      s->prof_bytes[f] = 0;
+    }
+  }
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_profile_read(ppvm_sum* s, char* names, size_t names_cap, double* ms, uint64_t* launches,
+                              uint64_t* bytes, size_t cap, size_t* n_out) {
+  if (!s || !n_out) return fail(PPVM_EINVAL, "null argument");
+  *n_out = F_COUNT;
+  std::string all;
+  for (int f = 0; f < F_COUNT; ++f) {
+    all += kFamilyNames[f];
+    all.push_back('\0');
+  }
+  if (names && names_cap) std::memcpy(names, all.data(), std::min(names_cap, all.size()));
+  for (size_t f = 0; f < std::min<size_t>(cap, F_COUNT); ++f) {
+    if (ms) ms[f] = s->prof_ms[f];
+    if (launches) launches[f] = s->prof_launches[f];
+    if (bytes) bytes[f] = s->prof_bytes[f];
+  }
+  return PPVM_OK;
+}
+
+}  // extern "C"
