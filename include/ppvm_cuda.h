@@ -169,6 +169,24 @@ ppvm_status ppvm_trace(ppvm_sum* sum, const char* pattern, double* out);
 /* PauliSum::overlap (crates/ppvm-pauli-sum/src/sum/trace.rs:31-37): sum_k a[k] * b[k]. */
 ppvm_status ppvm_overlap(ppvm_sum* a, ppvm_sum* b, double* out);
 
+/* overlap_with_zero for terms the caller already holds in device memory, for callers that
+ * cannot let a library allocate device memory: frameworks whose own pool owns the GPU's
+ * memory, or latency-critical loops where cudaMalloc/cudaFree would stall the device.
+ * No counterpart in the reference; it computes what ppvm_overlap_with_zero computes.
+ *   d_x      X plane words, word w of term i at d_x[w * x_stride + i] (x_stride >= n_terms)
+ *   n_words  words per plane, 1..8 (up to 512 qubits)
+ *   d_c      n_terms coefficients;  d_out  one double, written with the sum
+ *   cuda_stream  stream the work is queued on (NULL: the default stream); asynchronous
+ * Allocates nothing: its working memory is a fixed 32 KiB array compiled into the library,
+ * held on every GPU that loads the library until the process exits.  Limit: n_terms <=
+ * 16,777,216 (one partial sum per 4096 terms); larger inputs return PPVM_EINVAL.  The first
+ * call on each device looks up that array's device address; make that first call before any
+ * stream capture.  All calls on a device share the array: calls whose kernels overlap on
+ * the GPU (unordered streams) race and may return wrong sums. */
+ppvm_status ppvm_overlap_with_zero_noalloc(const uint64_t* d_x, size_t x_stride, uint32_t n_words,
+                                           const double* d_c, size_t n_terms, double* d_out,
+                                           void* cuda_stream);
+
 /* ---- fused gate lists ---------------------------------------------------------------- */
 /* Runs ops[0..n_ops) in order; PPVM_OP_TRUNCATE marks where the strategy runs.  Consecutive
  * Clifford ops are fused into one device pass.  Equivalent to calling the per-gate

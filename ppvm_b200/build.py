@@ -1,8 +1,7 @@
 """Build recipe of the CUDA library (sm_100a), used by __graft_entry__.build().
 
-The library is built in-tree as ppvm_b200/libppvm_cuda.so with nvcc directly: one
-translation unit (csrc/engine.cu) holding the kernels and the C ABI of
-include/ppvm_cuda.h.  -fmad=false keeps every coefficient product and sum a separately
+The library is built in-tree as ppvm_b200/libppvm_cuda.so with nvcc directly from
+csrc/engine.cu (the kernels and the C ABI of include/ppvm_cuda.h) and csrc/noalloc.cu.  -fmad=false keeps every coefficient product and sum a separately
 rounded IEEE operation, as the reference's f64 arithmetic is.
 """
 
@@ -15,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libppvm_cuda.so")
-SOURCES = [os.path.join(HERE, "csrc", "engine.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "engine.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "kernels.cuh")] + [
     os.path.join(ROOT, "include", "ppvm_cuda.h")
 ]

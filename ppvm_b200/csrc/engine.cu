@@ -81,6 +81,11 @@ const char* kFamilyNames[F_COUNT] = {"rot_scan", "rot_pair", "rot_apply", "rot_c
 
 }  // namespace
 
+namespace ppvm {
+// Lets other translation units of the library set the text of ppvm_last_error_string().
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace ppvm
+
 struct ppvm_sum {
   int device = 0;
   cudaStream_t stream = nullptr;
