@@ -70,6 +70,9 @@ typedef struct ppvm_op {
 /* Sum creation options (bit flags for ppvm_sum_create2). */
 #define PPVM_FLAG_CLIFFORD_ANGLES 1u /* treat Pauli rotations at theta = +-pi/2 as the
                                         Clifford they equal (cos = 0, sin = +-1 exactly) */
+#define PPVM_FLAG_EXACT_ORDER 2u     /* keep the reference's term order (IndexMap insertion
+                                        order) through every op: disables fused rotation runs,
+                                        which reorder terms (same terms, same coefficients) */
 
 /* ---- lifetime ------------------------------------------------------------------ */
 

@@ -16,6 +16,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "ppvm_cuda.h")
 
 OK, EINVAL, ECAPACITY, ECUDA, ETIMEOUT, ENODEV = range(6)
 FLAG_CLIFFORD_ANGLES = 1
+FLAG_EXACT_ORDER = 2
 UMAX = (1 << 64) - 1
 
 

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <set>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -17,7 +18,7 @@
 #include <vector>
 
 #include "../../include/ppvm_cuda.h"
-#include "kernels.cuh"
+#include "runs.cuh"
 
 using namespace ppvm;
 
@@ -75,9 +76,14 @@ struct ProfLaunch {
   cudaEvent_t a, b;
 };
 
-enum Family { F_SCAN = 0, F_PAIR, F_APPLY, F_COMMIT, F_CLIFF, F_TRUNC, F_READ, F_COUNT };
+enum Family {
+  F_SCAN = 0, F_PAIR, F_APPLY, F_COMMIT, F_CLIFF, F_TRUNC, F_READ,
+  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_UNTOUCHED, F_RUN_GROUPS, F_RUN_COMMIT, F_COUNT
+};
 const char* kFamilyNames[F_COUNT] = {"rot_scan", "rot_pair", "rot_apply", "rot_commit",
-                                     "clifford", "truncate", "readout"};
+                                     "clifford", "truncate", "readout",
+                                     "run_classify", "run_order", "run_scatter", "run_untouched",
+                                     "run_groups", "run_commit"};
 
 }  // namespace
 
@@ -100,6 +106,12 @@ struct ppvm_sum {
   unsigned long long n_ub = 0;    // upper bound of the live count (sizes grids)
 
   uint64_t* planes = nullptr;  // x[W*cap] z[W*cap] c[cap]
+  uint64_t* alt = nullptr;     // second plane buffer: fused runs write here, then swap
+  RunScratch R = {};
+  RunDesc* d_rundesc = nullptr;
+  unsigned long long* tstate2 = nullptr;
+  std::vector<int> swaps;      // op indices of fused runs enqueued in the current attempt
+  std::set<size_t> no_fuse;    // run starts that must take the per-gate path
   uint32_t* s_idx = nullptr;
   uint64_t* s_rec = nullptr;
   uint32_t* partner = nullptr;
@@ -130,21 +142,25 @@ struct ppvm_sum {
 
   bool prof = false;
   std::vector<ProfLaunch> prof_pending;
+  std::vector<cudaEvent_t> event_pool;  // reused profiling events
   double prof_ms[F_COUNT] = {};
   uint64_t prof_launches[F_COUNT] = {};
   uint64_t prof_bytes[F_COUNT] = {};
 
-  Planes planes_view() const {
+  Planes view_of(uint64_t* base) const {
     Planes p;
-    p.x = planes;
-    p.z = planes + (size_t)W * cap;
-    p.c = reinterpret_cast<double*>(planes + (size_t)2 * W * cap);
+    p.x = base;
+    p.z = base + (size_t)W * cap;
+    p.c = reinterpret_cast<double*>(base + (size_t)2 * W * cap);
     p.cap = cap;
     return p;
   }
+  Planes planes_view() const { return view_of(planes); }
+  Planes alt_view() const { return view_of(alt); }
   unsigned next_tile_epoch() {
     if (++tile_epoch >= 0xFFFFFu) {
       cudaMemsetAsync(tstate, 0, tstate_cap * sizeof(unsigned long long), stream);
+      cudaMemsetAsync(tstate2, 0, tstate_cap * sizeof(unsigned long long), stream);
       tile_epoch = 1;
     }
     return tile_epoch;
@@ -178,6 +194,15 @@ ppvm_status ensure_device(int dev) {
 }
 
 void free_scratch(ppvm_sum* s) {
+  cudaFree(s->alt);
+  cudaFree(s->tstate2);
+  uint32_t* run_arrays[] = {s->R.gslot, s->R.grp_min, s->R.grp_cnt, s->R.grp_ord, s->R.g_start,
+                            s->R.g_cnt, s->R.g_rep, s->R.g_fill, s->R.members};
+  for (uint32_t* p : run_arrays) cudaFree(p);
+  cudaFree(s->R.created);
+  s->R = RunScratch{};
+  s->alt = nullptr;
+  s->tstate2 = nullptr;
   cudaFree(s->s_idx);
   cudaFree(s->s_rec);
   cudaFree(s->partner);
@@ -216,7 +241,20 @@ ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   s->tstate_cap = new_cap / 512 + 64;
   CUDA_TRY(cudaMalloc(&s->tstate, sizeof(unsigned long long) * s->tstate_cap));
   CUDA_TRY(cudaMemsetAsync(s->tstate, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
+  CUDA_TRY(cudaMalloc(&s->tstate2, sizeof(unsigned long long) * s->tstate_cap));
+  CUDA_TRY(cudaMemsetAsync(s->tstate2, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
   s->tile_epoch = 0;
+  CUDA_TRY(cudaMalloc(&s->alt, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->R.gslot, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->R.grp_min, sizeof(uint32_t) * s->table_cap));
+  CUDA_TRY(cudaMalloc(&s->R.grp_cnt, sizeof(uint32_t) * s->table_cap));
+  CUDA_TRY(cudaMalloc(&s->R.grp_ord, sizeof(uint32_t) * s->table_cap));
+  CUDA_TRY(cudaMalloc(&s->R.g_start, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->R.g_cnt, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->R.g_rep, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->R.g_fill, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->R.members, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(cudaMalloc(&s->R.created, sizeof(unsigned long long) * kRunMaxGates));
   return PPVM_OK;
 }
 
@@ -251,14 +289,24 @@ struct ProfScope {
     L.family = family;
     L.op = op;
     L.nops = nops;
-    cudaEventCreate(&L.a);
-    cudaEventCreate(&L.b);
+    L.a = take();
+    L.b = take();
     cudaEventRecord(L.a, s->stream);
   }
   ~ProfScope() {
     if (!on) return;
     cudaEventRecord(L.b, s->stream);
     s->prof_pending.push_back(L);
+  }
+  cudaEvent_t take() {
+    if (s->event_pool.empty()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      return e;
+    }
+    cudaEvent_t e = s->event_pool.back();
+    s->event_pool.pop_back();
+    return e;
   }
 };
 
@@ -275,6 +323,12 @@ uint64_t launch_bytes(const ppvm_sum* s, const ProfLaunch& L, const std::vector<
     case F_APPLY: return g.n_s * (B + 8) + g.n_new * B;  // records, coeff writes, children
     case F_CLIFF: return 2ull * g.n_in * B;
     case F_TRUNC: return g.n_in * B + g.n_out * B;
+    case F_RUN_CLASSIFY: return g.n_in * B;                    // every term's key read once
+    case F_RUN_UNTOUCHED: return g.n_in * 8 + g.n_in * B;      // group slots + untouched terms
+    case F_RUN_GROUPS: {                                       // members read, group outputs written
+      const OpLog& last = s->h_log[L.op + std::max(L.nops, 1) - 1];
+      return g.n_s * B + (L.nops > 1 ? last.n_s : 0) * B;
+    }
     default: return 0;
   }
 }
@@ -286,8 +340,8 @@ void prof_collect(ppvm_sum* s, const std::vector<int>& test_words) {
     s->prof_ms[L.family] += ms;
     s->prof_launches[L.family] += 1;
     if (L.op >= 0 && (size_t)L.op < s->log_cap) s->prof_bytes[L.family] += launch_bytes(s, L, test_words);
-    cudaEventDestroy(L.a);
-    cudaEventDestroy(L.b);
+    s->event_pool.push_back(L.a);
+    s->event_pool.push_back(L.b);
   }
   s->prof_pending.clear();
 }
@@ -444,6 +498,54 @@ struct K {
     k_commit_truncate<W><<<1, 256, 0, s->stream>>>(P, s->d_ctrl, s->side, op, s->d_log);
   }
 
+  // Fused run of single-qubit RX (cls 0) or RZ (cls 1) rotations, ops[op0..op0+L), optionally
+  // followed by its TRUNCATE (trunc_op >= 0).  Writes into the alternate planes, then swaps.
+  static ppvm_status run(ppvm_sum* s, const RunDesc& rd, int op0, int L, int trunc_op) {
+    const Planes P = s->planes_view(), O = s->alt_view();
+    const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
+    unsigned long long tsize = next_pow2(std::max<unsigned long long>(2 * nub, 1024));
+    if (tsize > s->table_cap) tsize = s->table_cap;
+    CUDA_TRY(cudaMemcpyAsync(s->d_rundesc, &rd, sizeof(RunDesc), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->R.grp_min, 0xFF, sizeof(uint32_t) * tsize, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->R.grp_cnt, 0, sizeof(uint32_t) * tsize, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->R.created, 0, sizeof(unsigned long long) * kRunMaxGates, s->stream));
+    const int trunc = trunc_op >= 0 ? 1 : 0;
+    {
+      ProfScope ps(s, F_RUN_CLASSIFY, op0, L);
+      k_run_classify<W><<<grid_for(nub, 256, 8), 256, 0, s->stream>>>(P, s->d_ctrl, s->d_rundesc, s->R, s->table,
+                                                                       tsize - 1, s->next_table_epoch(), op0);
+    }
+    {
+      ProfScope ps(s, F_RUN_ORDER, op0, L);
+      const unsigned ea = s->next_tile_epoch(), eb = s->next_tile_epoch();
+      k_run_order<kScanBlock, 8><<<grid_for(nub, kScanBlock * 8, 8), kScanBlock, 0, s->stream>>>(
+          s->d_ctrl, s->R, s->tstate, s->tstate2, ea, eb, op0);
+    }
+    {
+      ProfScope ps(s, F_RUN_SCATTER, op0, L);
+      k_run_scatter<<<grid_for(nub, 256, 8), 256, 0, s->stream>>>(s->d_ctrl, s->R);
+    }
+    {
+      ProfScope ps(s, F_RUN_UNTOUCHED, op0, L);
+      k_run_untouched<W, kScanBlock, ITEMS><<<grid_for(nub, TILE, 8), kScanBlock, 0, s->stream>>>(
+          P, O, s->d_ctrl, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0);
+    }
+    {
+      ProfScope ps(s, F_RUN_GROUPS, op0, L);
+      k_run_groups<W><<<grid_for(nub, kRunWarps, 8), kRunWarps * 32, 0, s->stream>>>(
+          P, O, s->d_ctrl, s->d_rundesc, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0);
+    }
+    {
+      ProfScope ps(s, F_RUN_COMMIT, op0, L);
+      k_run_commit<<<1, 1, 0, s->stream>>>(s->d_ctrl, s->R, op0, L, trunc_op, s->d_log);
+    }
+    std::swap(s->planes, s->alt);
+    s->swaps.push_back(op0);
+    const int grow_bits = std::min(L, kRunMaxK);
+    s->n_ub = std::min<unsigned long long>(s->cap, s->n_ub << grow_bits);
+    return PPVM_OK;
+  }
+
   static void owz(ppvm_sum* s, int nblocks) {
     k_owz<W><<<nblocks, kRedBlock, 0, s->stream>>>(s->planes_view(), s->d_ctrl, s->d_partials);
     k_sum_partials<<<1, kRedBlock, 0, s->stream>>>(s->d_partials, nblocks, s->d_ctrl);
@@ -485,6 +587,22 @@ struct K {
     case 7: K<7>::CALL; break;               \
     default: K<8>::CALL; break;              \
   }
+
+#define DISPATCH_W_RET(W_, CALL)                   \
+  switch (W_) {                                    \
+    case 1: return K<1>::CALL;                     \
+    case 2: return K<2>::CALL;                     \
+    case 3: return K<3>::CALL;                     \
+    case 4: return K<4>::CALL;                     \
+    case 5: return K<5>::CALL;                     \
+    case 6: return K<6>::CALL;                     \
+    case 7: return K<7>::CALL;                     \
+    default: return K<8>::CALL;                    \
+  }
+
+ppvm_status enqueue_run(ppvm_sum* s, const RunDesc& rd, int op0, int L, int trunc_op) {
+  DISPATCH_W_RET(s->W, run(s, rd, op0, L, trunc_op));
+}
 
 int test_words_of(int W, const Gen& g) {
   int n = 0;
@@ -552,6 +670,33 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
       run.push_back(to_devop(op));
       continue;
     }
+    // fused run of single-qubit RX (or RZ) rotations on distinct qubits
+    const bool fusable = (op.code == PPVM_OP_RX || op.code == PPVM_OP_RZ) &&
+                         !(s->flags & PPVM_FLAG_EXACT_ORDER) && s->npres == 0 && !s->no_fuse.count(i);
+    if (fusable) {
+      RunDesc rd;
+      std::memset(&rd, 0, sizeof(rd));
+      rd.cls = op.code == PPVM_OP_RX ? 0 : 1;
+      size_t j = i;
+      while (j < n_ops && (int)(j - i) < kRunMaxGates) {
+        const ppvm_op& o = ops[j];
+        if (o.flags != 0 || o.code != op.code || is_clifford_angle(s, o.theta)) break;
+        if ((rd.Q[o.q0 >> 6] >> (o.q0 & 63)) & 1ull) break;  // qubit repeats: end the run
+        rd.Q[o.q0 >> 6] |= 1ull << (o.q0 & 63);
+        rd.q[rd.L] = o.q0;
+        rd.sn[rd.L] = std::sin(o.theta);
+        rd.cs[rd.L] = std::cos(o.theta);
+        ++rd.L;
+        ++j;
+      }
+      if (rd.L >= 2) {
+        PPVM_TRY(flush());
+        const int trunc_op = (j < n_ops && ops[j].code == PPVM_OP_TRUNCATE && ops[j].flags == 0) ? (int)j : -1;
+        PPVM_TRY(enqueue_run(s, rd, (int)i, (int)rd.L, trunc_op));
+        i = trunc_op >= 0 ? j : j - 1;  // the loop's ++i moves past the run (and its TRUNCATE)
+        continue;
+      }
+    }
     PPVM_TRY(flush());
     Gen g;
     gen_from_op(s, op, g);
@@ -570,7 +715,9 @@ ppvm_status run_list(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, const std::v
   PPVM_TRY(ensure_log(s, std::max<size_t>(n_ops, 1)));
   std::vector<int> test_words(n_ops, 0);
   size_t start = 0;
+  s->no_fuse.clear();
   for (int attempt = 0; attempt < 64; ++attempt) {
+    s->swaps.clear();
     PPVM_TRY(enqueue(s, ops, n_ops, start, gens, test_words));
     PPVM_TRY(sync_state(s, n_ops));
     const Ctrl& c = *s->h_ctrl;
@@ -582,6 +729,16 @@ ppvm_status run_list(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, const std::v
       return PPVM_OK;
     }
     if (s->prof) prof_collect(s, test_words);
+    // fused runs at or after the failing op did not run: give their buffers back
+    for (int op0 : s->swaps)
+      if (op0 >= c.err_op) std::swap(s->planes, s->alt);
+    if (c.err == kErrFallback && c.err_op >= 0 && (size_t)c.err_op >= start) {
+      start = (size_t)c.err_op;
+      s->no_fuse.insert(start);
+      PPVM_TRY(clear_err(s));
+      s->n_ub = s->n_host;
+      continue;
+    }
     if (c.err == kErrCapacity && c.err_op >= 0 && (size_t)c.err_op >= start) {
       const unsigned long long need = c.cap_needed;
       start = (size_t)c.err_op;
@@ -749,6 +906,7 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
       cudaMalloc(&s->d_ops, sizeof(DevOp) * kMaxOpsPerLaunch) != cudaSuccess ||
       cudaMalloc(&s->d_partials, sizeof(double) * 8192) != cudaSuccess ||
       cudaMalloc(&s->d_counter, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&s->d_rundesc, sizeof(RunDesc)) != cudaSuccess ||
       cudaMalloc(&s->side, sizeof(uint64_t) * (2 * s->W + 1) * (kMaxPreserve + 1)) != cudaSuccess)
     return bail(fail(PPVM_ECAPACITY, "device allocation failed"));
   std::memset(s->h_ctrl, 0, sizeof(Ctrl));
@@ -776,6 +934,7 @@ ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
     cudaEventDestroy(L.a);
     cudaEventDestroy(L.b);
   }
+  for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
   cudaFree(s->planes);
   free_scratch(s);
   cudaFree(s->side);
@@ -787,6 +946,7 @@ ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
   cudaFree(s->d_pat);
   cudaFree(s->d_partials);
   cudaFree(s->d_counter);
+  cudaFree(s->d_rundesc);
   cudaFree(s->d_pres_keys);
   cudaFree(s->d_pres_table);
   if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);

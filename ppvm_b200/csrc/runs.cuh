@@ -1,0 +1,500 @@
+// runs.cuh — fused runs of single-qubit X-type or Z-type rotations.
+//
+// A run is a sequence of RX rotations on distinct qubits (or of RZ rotations on distinct
+// qubits) with no other op in between, optionally ending in TRUNCATE.  During such a run a
+// term's Z plane (RX) or X plane (RZ) never changes: it is the invariant plane v.  Gate j on
+// qubit q acts on a term iff v has bit q, and then only flips bit q of the other plane f.
+// So the terms sharing (v, f with the bits M = v & Q cleared) — Q the run's qubits — form a
+// group that evolves on its own: its members are the 2^|M| words f0 | pdep(c, M), c in
+// [0, 2^|M|).  The reference processes the run gate by gate over the whole map
+// (PauliSum::map_insert per gate, crates/ppvm-pauli-sum/src/sum/data.rs:204-226); here each
+// group is loaded once, the gates of the run are applied in the same order with the same
+// arithmetic as a butterfly over coordinates c in shared memory (existence tracked
+// separately from the coefficient, as a map entry exists even with coefficient 0), and the
+// truncation that ends the run is applied before anything is written back.  The term set
+// and every coefficient are identical to the reference's; only the output order differs
+// (untouched terms in order, then groups by their first member, members by coordinate).
+//
+// Kernels, in order: k_run_classify (group keys into a hash table, members counted),
+// k_run_order (deterministic group numbering by first member, member offsets),
+// k_run_scatter (member lists), k_run_untouched (terms outside every group, compacted),
+// k_run_groups (butterfly + truncation + ordered write), k_run_commit (counts, op log).
+#pragma once
+
+#include "kernels.cuh"
+
+namespace ppvm {
+
+constexpr int kRunMaxK = 10;       // groups up to 2^10 coordinates in shared memory
+constexpr int kRunMaxGates = 256;  // gates per fused run
+constexpr int kRunWarps = 4;       // groups per block tile
+constexpr int kErrFallback = 4;    // device error: a group exceeds kRunMaxK; rerun per gate
+
+struct RunDesc {
+  uint32_t cls;   // 0: RX run (v = z plane, f = x plane); 1: RZ run (v = x, f = z)
+  uint32_t L;     // gates
+  uint64_t Q[kMaxW];
+  uint32_t q[kRunMaxGates];
+  double sn[kRunMaxGates];
+  double cs[kRunMaxGates];
+};
+
+struct RunScratch {
+  uint32_t* gslot;     // per term: group slot (kNone = untouched)
+  uint32_t* grp_min;   // per table slot: smallest member index
+  uint32_t* grp_cnt;   // per table slot: member count
+  uint32_t* grp_ord;   // per table slot: group ordinal
+  uint32_t* g_start;   // per group
+  uint32_t* g_cnt;
+  uint32_t* g_rep;
+  uint32_t* g_fill;
+  uint32_t* members;
+  unsigned long long* created;  // per gate of the run: children created
+};
+
+template <int W>
+__device__ __forceinline__ void split_planes(uint32_t cls, const uint64_t (&x)[W], const uint64_t (&z)[W],
+                                             uint64_t (&v)[W], uint64_t (&f)[W]) {
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    v[w] = cls == 0 ? z[w] : x[w];
+    f[w] = cls == 0 ? x[w] : z[w];
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+template <int W>
+__global__ void __launch_bounds__(256)
+k_run_classify(Planes P, Ctrl* ctrl, const RunDesc* rd, RunScratch R, unsigned long long* table,
+               unsigned long long tmask, unsigned tepoch, int op) {
+  if (ld_volatile_int(&ctrl->err)) return;
+  const unsigned long long N = ld_volatile(&ctrl->n);
+  const uint32_t cls = rd->cls;
+  uint64_t Q[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) Q[w] = rd->Q[w];
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    uint64_t x[W], z[W], v[W], f[W], M[W];
+    load_key<W>(P, i, x, z);
+    split_planes<W>(cls, x, z, v, f);
+    unsigned k = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      M[w] = v[w] & Q[w];
+      k += __popcll(M[w]);
+      f[w] &= ~M[w];
+    }
+    if (k == 0) {
+      R.gslot[i] = kNone;
+      continue;
+    }
+    if (k > (unsigned)kRunMaxK) {
+      set_err(ctrl, kErrFallback, op);
+      R.gslot[i] = kNone;
+      continue;
+    }
+    const uint64_t h = hash_key<W>(v, f);
+    const unsigned tag = (unsigned)(h >> 48) & 0xFFFFu;
+    const unsigned long long mine = make_slot(tepoch, tag, (unsigned)i);
+    unsigned long long slot = h & tmask;
+    unsigned long long probes = 0;
+    while (true) {
+      const unsigned long long cur = ld_volatile(&table[slot]);
+      if (slot_epoch(cur) != (tepoch & 0xFFFFu)) {
+        const unsigned long long prev = atomicCAS(&table[slot], cur, mine);
+        if (prev != cur) continue;
+        break;  // new group
+      }
+      if (slot_tag(cur) == tag) {
+        uint64_t jx[W], jz[W], jv[W], jf[W];
+        load_key<W>(P, slot_idx(cur), jx, jz);
+        split_planes<W>(cls, jx, jz, jv, jf);
+        bool eq = true;
+#pragma unroll
+        for (int w = 0; w < W; ++w) eq &= (jv[w] == v[w]) & ((jf[w] & ~M[w]) == f[w]);
+        if (eq) break;  // same group
+      }
+      slot = (slot + 1) & tmask;
+      if (++probes > tmask) {
+        set_err(ctrl, kErrProbe, op);
+        break;
+      }
+    }
+    R.gslot[i] = (uint32_t)slot;
+    atomicMin(&R.grp_min[slot], (uint32_t)i);
+    atomicAdd(&R.grp_cnt[slot], 1u);
+  }
+}
+
+// Numbers the groups by their smallest member (index order) and lays out member lists.
+template <int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK)
+k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long long* ts_b, unsigned ep_a,
+            unsigned ep_b, int op) {
+  __shared__ unsigned s_tile;
+  __shared__ unsigned long long s_slot;
+  __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
+  __shared__ unsigned long long s_cnt[BLOCK];
+  if (ld_volatile_int(&ctrl->err)) return;
+  const unsigned long long N = ld_volatile(&ctrl->n);
+  constexpr unsigned long long TILE = (unsigned long long)BLOCK * ITEMS;
+  const unsigned long long ntiles = (N + TILE - 1) / TILE;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && N == 0) {
+    ctrl->n_pairs = 0;   // groups
+    ctrl->n_side = 0;    // members
+  }
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = BLOCK / 32;
+  for (;;) {
+    const unsigned tile = next_tile(&ctrl->tickets[0], &s_tile);
+    if (tile >= ntiles) break;
+    const unsigned long long base = (unsigned long long)tile * TILE;
+    unsigned ballots[ITEMS];
+    unsigned cnts[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
+      bool rep = false;
+      cnts[k] = 0;
+      if (i < N) {
+        const uint32_t s = R.gslot[i];
+        if (s != kNone && R.grp_min[s] == (uint32_t)i) {
+          rep = true;
+          cnts[k] = R.grp_cnt[s];
+        }
+      }
+      ballots[k] = __ballot_sync(kFull, rep);
+    }
+    const unsigned agg = tile_ranks<BLOCK, ITEMS>(ballots, s_base);
+    // member-count prefix in index order: per item k, warp-level scan, then across (k, warp)
+    // The per-(k,warp) sums are small; a second rank table over counts is built in s_cnt.
+    unsigned long long item_pre[ITEMS];
+    unsigned long long warp_tot[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      unsigned long long v = cnts[k];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(kFull, v, o);
+        if (lane >= (unsigned)o) v += t;
+      }
+      item_pre[k] = v - cnts[k];
+      warp_tot[k] = __shfl_sync(kFull, v, 31);
+    }
+    // s_cnt[k*NW + warp] = warp totals; exclusive scan by thread 0 (ITEMS*NW <= 64 entries)
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < ITEMS; ++k) s_cnt[k * NW + warp] = warp_tot[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long run = 0;
+      for (int e = 0; e < ITEMS * NW; ++e) {
+        const unsigned long long t = s_cnt[e];
+        s_cnt[e] = run;
+        run += t;
+      }
+      s_cnt[ITEMS * NW] = run;
+    }
+    __syncthreads();
+    const unsigned long long agg_cnt = s_cnt[ITEMS * NW];
+    const unsigned long long excl = lookback(ts_a, tile, agg, ep_a, ctrl, op, &s_slot);
+    const unsigned long long excl_cnt = lookback(ts_b, tile, agg_cnt, ep_b, ctrl, op, &s_slot);
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      if ((ballots[k] >> lane) & 1u) {
+        const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
+        const unsigned long long ord = excl + s_base[k * NW + warp] + __popc(ballots[k] & ((1u << lane) - 1u));
+        const unsigned long long start = excl_cnt + s_cnt[k * NW + warp] + item_pre[k];
+        const uint32_t s = R.gslot[i];
+        R.grp_ord[s] = (uint32_t)ord;
+        R.g_start[ord] = (uint32_t)start;
+        R.g_cnt[ord] = cnts[k];
+        R.g_rep[ord] = (uint32_t)i;
+        R.g_fill[ord] = 0;
+      }
+    }
+    if (tile == ntiles - 1 && threadIdx.x == 0) {
+      ctrl->n_pairs = excl + agg;        // groups
+      ctrl->n_side = excl_cnt + agg_cnt; // members (touched terms)
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_run_scatter(Ctrl* ctrl, RunScratch R) {
+  if (ld_volatile_int(&ctrl->err)) return;
+  const unsigned long long N = ld_volatile(&ctrl->n);
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t s = R.gslot[i];
+    if (s == kNone) continue;
+    const uint32_t o = R.grp_ord[s];
+    const uint32_t pos = R.g_start[o] + atomicAdd(&R.g_fill[o], 1u);
+    R.members[pos] = (uint32_t)i;
+  }
+}
+
+// Terms outside every group: unchanged by the run; compacted (with the truncation that ends
+// the run, if any) to the front of the output planes, in index order.
+template <int W, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK)
+k_run_untouched(Planes P, Planes O, Ctrl* ctrl, RunScratch R, int trunc, double thr, unsigned long long maxw,
+                unsigned long long* ts, unsigned epoch, int op) {
+  __shared__ unsigned s_tile;
+  __shared__ unsigned long long s_slot;
+  __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
+  if (ld_volatile_int(&ctrl->err)) return;
+  const unsigned long long N = ld_volatile(&ctrl->n);
+  constexpr unsigned long long TILE = (unsigned long long)BLOCK * ITEMS;
+  const unsigned long long ntiles = (N + TILE - 1) / TILE;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && N == 0) ctrl->n_s = 0;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = BLOCK / 32;
+  const bool wcap = maxw != ~0ull;
+  for (;;) {
+    const unsigned tile = next_tile(&ctrl->tickets[1], &s_tile);
+    if (tile >= ntiles) break;
+    const unsigned long long base = (unsigned long long)tile * TILE;
+    unsigned ballots[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
+      bool keep = false;
+      if (i < N && R.gslot[i] == kNone) {
+        keep = true;
+        if (trunc) {
+          uint64_t x[W], z[W];
+          load_key<W>(P, i, x, z);
+          keep = !(fabs(P.c[i]) < thr);
+          if (wcap) keep = keep && (weight<W>(x, z) <= maxw);
+        }
+      }
+      ballots[k] = __ballot_sync(kFull, keep);
+    }
+    const unsigned agg = tile_ranks<BLOCK, ITEMS>(ballots, s_base);
+    const unsigned long long excl = lookback(ts, tile, agg, epoch, ctrl, op, &s_slot);
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      if ((ballots[k] >> lane) & 1u) {
+        const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
+        const unsigned long long r = excl + s_base[k * NW + warp] + __popc(ballots[k] & ((1u << lane) - 1u));
+        uint64_t x[W], z[W];
+        load_key<W>(P, i, x, z);
+        store_key<W>(O, r, x, z);
+        O.c[r] = P.c[i];
+      }
+    }
+    if (tile == ntiles - 1 && threadIdx.x == 0) ctrl->n_s = excl + agg;
+  }
+}
+
+// One warp per group: butterfly over the group's coordinates, gates in run order.
+template <int W>
+__global__ void __launch_bounds__(kRunWarps * 32)
+k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, int trunc, double thr,
+             unsigned long long maxw, unsigned long long* ts, unsigned epoch, int op) {
+  constexpr int SZ = 1 << kRunMaxK;
+  __shared__ double s_coef[kRunWarps][SZ];
+  __shared__ unsigned s_ex[kRunWarps][SZ / 32];
+  __shared__ unsigned s_cnt[kRunWarps + 1];
+  __shared__ unsigned s_tile;
+  __shared__ unsigned long long s_slot;
+  __shared__ unsigned long long s_created[kRunMaxGates];
+  if (ld_volatile_int(&ctrl->err)) return;
+  const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs);
+  const unsigned long long ubase = ld_volatile(&ctrl->n_s);  // untouched survivors go first
+  const uint32_t cls = rd->cls;
+  const uint32_t L = rd->L;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (unsigned j = threadIdx.x; j < L; j += blockDim.x) s_created[j] = 0;
+  __syncthreads();
+  const unsigned long long ntiles = (ngroups + kRunWarps - 1) / kRunWarps;
+  const bool wcap = maxw != ~0ull;
+  double* coef = s_coef[warp];
+  unsigned* ex = s_ex[warp];
+  for (;;) {
+    const unsigned tile = next_tile(&ctrl->tickets[2], &s_tile);
+    if (tile >= ntiles) break;
+    const unsigned long long g = (unsigned long long)tile * kRunWarps + warp;
+    const bool active = g < ngroups;
+    uint64_t v[W], f0[W], M[W];
+    unsigned k = 0, size = 0;
+    uint16_t pos[kRunMaxK];  // qubit of coordinate bit t (ascending)
+    bool wok = true;
+    if (active) {
+      const uint32_t rep = R.g_rep[g];
+      uint64_t x[W], z[W], f[W];
+      load_key<W>(P, rep, x, z);
+      split_planes<W>(cls, x, z, v, f);
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        M[w] = v[w] & rd->Q[w];
+        f0[w] = f[w] & ~M[w];
+      }
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        uint64_t m = M[w];
+        while (m) {
+          const int b = __ffsll((long long)m) - 1;
+          pos[k++] = (uint16_t)(w * 64 + b);
+          m &= m - 1;
+        }
+      }
+      size = 1u << k;
+      if (wcap) {
+        unsigned wt = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) wt += __popcll(v[w] | f0[w]);
+        wok = wt <= maxw;  // M is inside v, so every member has this weight
+      }
+      for (unsigned e = lane; e < (size + 31) / 32; e += 32) ex[e] = 0u;
+      __syncwarp();
+      const uint32_t start = R.g_start[g], cnt = R.g_cnt[g];
+      for (uint32_t m = lane; m < cnt; m += 32) {
+        const uint32_t i = R.members[start + m];
+        unsigned c = 0;
+        for (unsigned t = 0; t < k; ++t) {
+          const unsigned q = pos[t];
+          const uint64_t fw = cls == 0 ? P.x[(unsigned long long)(q >> 6) * P.cap + i]
+                                       : P.z[(unsigned long long)(q >> 6) * P.cap + i];
+          c |= (unsigned)((fw >> (q & 63)) & 1ull) << t;
+        }
+        coef[c] = P.c[i];
+        atomicOr(&ex[c >> 5], 1u << (c & 31));
+      }
+      __syncwarp();
+      // gates of the run in order; eps of a member with bit t = b:
+      //   RX: eps = b ? -1 : +1   (crates/ppvm-pauli-sum/src/sum/rot1.rs:73)
+      //   RZ: eps = b ? +1 : -1   (rot1.rs:124)
+      const double eps_a = cls == 0 ? 1.0 : -1.0, eps_b = -eps_a;
+      for (uint32_t j = 0; j < L; ++j) {
+        const unsigned q = rd->q[j];
+        if (!((M[q >> 6] >> (q & 63)) & 1ull)) continue;
+        unsigned t = 0;
+        while (pos[t] != q) ++t;
+        const unsigned bit = 1u << t;
+        const double cs = rd->cs[j], sn = rd->sn[j];
+        unsigned made = 0;
+        for (unsigned p = lane; p < size / 2; p += 32) {
+          const unsigned a = ((p >> t) << (t + 1)) | (p & (bit - 1));
+          const unsigned b = a | bit;
+          const bool ea = (ex[a >> 5] >> (a & 31)) & 1u, eb = (ex[b >> 5] >> (b & 31)) & 1u;
+          if (ea && eb) {
+            const double ca = coef[a], cb = coef[b];
+            coef[a] = __dadd_rn(__dmul_rn(ca, cs), __dmul_rn(cb, eps_b * sn));
+            coef[b] = __dadd_rn(__dmul_rn(cb, cs), __dmul_rn(ca, eps_a * sn));
+          } else if (ea) {
+            const double ca = coef[a];
+            coef[a] = __dmul_rn(ca, cs);
+            coef[b] = __dmul_rn(ca, eps_a * sn);
+            atomicOr(&ex[b >> 5], 1u << (b & 31));
+            ++made;
+          } else if (eb) {
+            const double cb = coef[b];
+            coef[b] = __dmul_rn(cb, cs);
+            coef[a] = __dmul_rn(cb, eps_b * sn);
+            atomicOr(&ex[a >> 5], 1u << (a & 31));
+            ++made;
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int o = 16; o; o >>= 1) made += __shfl_down_sync(kFull, made, o);
+        if (lane == 0 && made) atomicAdd(&s_created[j], (unsigned long long)made);
+      }
+    }
+    // survivors, in coordinate order, counted per warp
+    unsigned mine = 0;
+    if (active) {
+      for (unsigned c = lane; c < size; c += 32) {
+        const bool e = (ex[c >> 5] >> (c & 31)) & 1u;
+        bool keep = e;
+        if (trunc && e) keep = wok && !(fabs(coef[c]) < thr);
+        mine += keep;
+      }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(kFull, mine, o);
+      mine = __shfl_sync(kFull, mine, 0);
+    }
+    if (lane == 0) s_cnt[warp] = active ? mine : 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned run = 0;
+      for (int w = 0; w < kRunWarps; ++w) {
+        const unsigned t = s_cnt[w];
+        s_cnt[w] = run;
+        run += t;
+      }
+      s_cnt[kRunWarps] = run;
+    }
+    __syncthreads();
+    const unsigned agg = s_cnt[kRunWarps];
+    const unsigned long long excl = lookback(ts, tile, agg, epoch, ctrl, op, &s_slot);
+    if (active) {
+      unsigned long long out = ubase + excl + s_cnt[warp];
+      for (unsigned c0 = 0; c0 < size; c0 += 32) {
+        const unsigned c = c0 + lane;
+        bool keep = false;
+        if (c < size) {
+          keep = (ex[c >> 5] >> (c & 31)) & 1u;
+          if (trunc && keep) keep = wok && !(fabs(coef[c]) < thr);
+        }
+        const unsigned bal = __ballot_sync(kFull, keep);
+        if (keep) {
+          const unsigned long long r = out + __popc(bal & ((1u << lane) - 1u));
+          if (r < O.cap) {
+            uint64_t f[W], x[W], z[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) f[w] = f0[w];
+            for (unsigned t = 0; t < k; ++t)
+              if ((c >> t) & 1u) f[pos[t] >> 6] |= 1ull << (pos[t] & 63);
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+              x[w] = cls == 0 ? f[w] : v[w];
+              z[w] = cls == 0 ? v[w] : f[w];
+            }
+            store_key<W>(O, r, x, z);
+            O.c[r] = coef[c];
+          }
+        }
+        out += __popc(bal);
+      }
+    }
+    if (tile == ntiles - 1 && threadIdx.x == 0) {
+      ctrl->cap_needed = ubase + excl + agg;
+      if (ubase + excl + agg > O.cap) set_err(ctrl, kErrCapacity, op);
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  for (unsigned j = threadIdx.x; j < L; j += blockDim.x)
+    if (s_created[j]) atomicAdd(&R.created[j], s_created[j]);
+}
+
+// Publishes the count after the run and fills the op log of its gates (and its TRUNCATE).
+__global__ void k_run_commit(Ctrl* ctrl, RunScratch R, int op0, int L, int trunc_op, OpLog* log) {
+  for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
+  if (ctrl->err) return;
+  const unsigned long long n0 = ctrl->n;
+  const unsigned long long ngroups = ctrl->n_pairs;
+  unsigned long long n = n0;
+  for (int j = 0; j < L; ++j) {
+    log[op0 + j].n_in = n;
+    log[op0 + j].n_new = R.created[j];
+    n += R.created[j];
+    log[op0 + j].n_out = n;
+    log[op0 + j].n_s = 0;
+  }
+  log[op0].n_s = ctrl->n_side;                               // touched terms (profiling bytes)
+  if (L > 1) log[op0 + L - 1].n_s = (ngroups == 0) ? 0 : ctrl->cap_needed - ctrl->n_s;  // group outputs
+  const unsigned long long out = (ngroups == 0) ? ctrl->n_s : ctrl->cap_needed;
+  if (trunc_op >= 0) {
+    log[trunc_op].n_in = n;
+    log[trunc_op].n_out = out;
+  }
+  ctrl->n = out;
+}
+
+}  // namespace ppvm

@@ -23,7 +23,7 @@ from typing import Any
 import numpy as np
 
 from . import gates as G
-from ._lib import EINVAL, FLAG_CLIFFORD_ANGLES, OK, UMAX, Op, PPVMError, lib
+from ._lib import EINVAL, FLAG_CLIFFORD_ANGLES, FLAG_EXACT_ORDER, OK, UMAX, Op, PPVMError, lib
 
 _COMPACT_RE = re.compile(r"^([IXYZ]\d+)+$")
 _COMPACT_TOKEN_RE = re.compile(r"([IXYZ])(\d+)")
@@ -89,14 +89,16 @@ class PauliSum:
     Attributes mirror the reference dataclass: ``initial_terms``, ``n_qubits``,
     ``coefficients``, ``min_abs_coeff`` (default 1e-10), ``max_pauli_weight`` (None = no cap),
     ``preserve_strings``.  Extra keyword-only options: ``clifford_angles`` (treat rotations
-    at +-pi/2 as the Clifford they equal), ``device`` (CUDA ordinal), ``capacity`` (initial
-    term capacity).
+    at +-pi/2 as the Clifford they equal), ``exact_order`` (keep the reference's term order
+    through every op; disables fused rotation runs, which give the same terms and coefficients
+    in another order), ``device`` (CUDA ordinal), ``capacity`` (initial term capacity).
     """
 
     def __init__(self, initial_terms: Sequence[str], n_qubits: int, coefficients: Sequence[float] = (),
                  min_abs_coeff: float = 1e-10, max_pauli_weight: int | None = None,
                  max_loss_weight: int | None = None, preserve_strings: Sequence[str] | None = None,
-                 *, clifford_angles: bool = False, device: int = 0, capacity: int = 0):
+                 *, clifford_angles: bool = False, exact_order: bool = False, device: int = 0,
+                 capacity: int = 0):
         if max_loss_weight is not None:
             raise NotImplementedError("lossy Pauli words are not supported by this engine")
         if not initial_terms:
@@ -119,7 +121,7 @@ class PauliSum:
         self.W = G.words(self.n_qubits)
         self._h = ctypes.c_void_p()
         mw = UMAX if max_pauli_weight is None else int(max_pauli_weight)
-        flags = FLAG_CLIFFORD_ANGLES if clifford_angles else 0
+        flags = (FLAG_CLIFFORD_ANGLES if clifford_angles else 0) | (FLAG_EXACT_ORDER if exact_order else 0)
         self._check(lib().ppvm_sum_create2(ctypes.byref(self._h), self.n_qubits, self.min_abs_coeff, mw,
                                            int(capacity), flags, int(device)))
         if self.preserve_strings:

@@ -1,9 +1,11 @@
 """GPU engine vs the CPU oracle, through the C ABI (ppvm_b200.PauliSum -> libppvm_cuda.so).
 
-The engine keeps the reference's term order (IndexMap order), so the bar is stricter than a
-sorted-multiset comparison: the exported term lists must be identical, word for word and
-coefficient bit for bit.  overlap_with_zero sums in a different order than the reference's
-sequential fold, so it is compared to 1e-10 absolute.
+Two modes are checked.  With ``exact_order`` the engine keeps the reference's term order
+(IndexMap order) and the exported term lists must be identical, word for word and
+coefficient bit for bit.  In the default mode fused rotation runs reorder terms, so the
+sorted term lists must be identical, again with every coefficient equal bit for bit.
+overlap_with_zero sums in a different order than the reference's sequential fold, so it is
+compared to 1e-10 absolute.
 """
 
 import json
@@ -22,10 +24,11 @@ pytestmark = pytest.mark.gpu
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_tables.json")))
 
 
-def gpu_from(terms, n, thr=1e-10, maxw=None, clifford_angles=False, capacity=0, preserve=None):
+def gpu_from(terms, n, thr=1e-10, maxw=None, clifford_angles=False, capacity=0, preserve=None,
+             exact=True):
     return PauliSum([t for t, _ in terms], n, [c for _, c in terms], min_abs_coeff=thr,
                     max_pauli_weight=maxw, preserve_strings=preserve, clifford_angles=clifford_angles,
-                    capacity=capacity)
+                    capacity=capacity, exact_order=exact)
 
 
 def same(gpu, orc):
@@ -38,15 +41,32 @@ def same(gpu, orc):
     assert bad.size == 0, (bad[:5], gc[bad[:5]], oc[bad[:5]])
 
 
-def run_both(terms, n, ops, thr=1e-10, maxw=None, clifford_angles=False, capacity=0, check_every=None):
-    g = gpu_from(terms, n, thr, maxw, clifford_angles, capacity)
+def _sorted(x, z, c):
+    keys = np.concatenate([x, z], axis=1)
+    order = np.lexsort(keys.T[::-1]) if len(c) else np.zeros(0, dtype=np.int64)
+    return keys[order], c[order]
+
+
+def same_set(gpu, orc):
+    """Identical term sets, every coefficient equal bit for bit (order free)."""
+    gk, gc = _sorted(*gpu.export())
+    ok, oc = _sorted(*orc.export())
+    assert gc.shape == oc.shape, (len(gc), len(oc))
+    assert np.array_equal(gk, ok)
+    bad = np.nonzero(gc.view(np.uint64) != oc.view(np.uint64))[0]
+    assert bad.size == 0, (bad[:5], gc[bad[:5]], oc[bad[:5]])
+
+
+def run_both(terms, n, ops, thr=1e-10, maxw=None, clifford_angles=False, capacity=0, check_every=None,
+             exact=True):
+    g = gpu_from(terms, n, thr, maxw, clifford_angles, capacity, exact=exact)
     o = oracle_from(terms, n, thr, maxw, clifford_angles)
     step = check_every or max(1, len(ops))
     for i in range(0, len(ops), step):
         chunk = ops[i:i + step]
         g.run(chunk)
         o.run_ops(chunk)
-        same(g, o)
+        (same if exact else same_set)(g, o)
     assert abs(g.overlap_with_zero() - o.overlap_with_zero()) < 1e-10
     return g, o
 
@@ -140,10 +160,31 @@ def random_case(n, seed):
     return list(terms.items()), _random_ops(rng, n, 160, hot)
 
 
+@pytest.mark.parametrize("exact", [True, False])
 @pytest.mark.parametrize("n", [5, 20, 64, 65, 100, 144, 200])
-def test_random_circuits(n):
+def test_random_circuits(n, exact):
     terms, ops = random_case(n, n)
-    g, _ = run_both(terms, n, ops, thr=1e-4, maxw=8, check_every=10)
+    g, _ = run_both(terms, n, ops, thr=1e-4, maxw=8, check_every=10, exact=exact)
+
+
+@pytest.mark.parametrize("n", [12, 70, 144, 200])
+def test_fused_rotation_runs(n):
+    # layers of RX on every qubit then RZ on every qubit (each a fused run ending in TRUNCATE),
+    # with Clifford layers in between; sparse random start terms
+    rng = np.random.default_rng(100 + n)
+    terms = {}
+    for _ in range(20):
+        w = ["I"] * n
+        for q in rng.choice(n, 3, replace=False):
+            w[int(q)] = "XYZ"[int(rng.integers(3))]
+        terms["".join(w)] = float(rng.uniform(-1, 1))
+    ops = []
+    for layer in range(3):
+        ops += [G.r1(G.RX, q, 0.3 + 0.01 * layer) for q in rng.permutation(n)] + [G.truncate()]
+        ops += [G.g2(G.CNOT, q, q + 1) for q in range(0, n - 1, 2)]
+        ops += [G.r1(G.RZ, q, -0.7) for q in range(n)]  # no TRUNCATE: run without a cut
+        ops += [G.g1(G.H, q) for q in range(0, n, 3)] + [G.truncate()]
+    run_both(list(terms.items()), n, ops, thr=1e-3, maxw=6, check_every=len(ops) // 3, exact=False)
 
 
 def test_capacity_growth_replay():
@@ -151,24 +192,27 @@ def test_capacity_growth_replay():
     # beyond the initial 4096-term capacity: rotations overflow, grow and replay.
     n = 14
     ops = [G.r1(G.RX, q, 0.3) for q in range(n)] + [G.r1(G.RZ, q, 0.4) for q in range(3)] + [G.truncate()]
-    g = gpu_from([("Z" * n, 1.0)], n, thr=1e-9, capacity=1)
-    o = oracle_from([("Z" * n, 1.0)], n, thr=1e-9)
-    g.run(ops)
-    o.run_ops(ops)
-    same(g, o)
-    assert len(g) > 4096
+    for exact in (True, False):  # fused: |M| = 14 > 10 falls back to the per-gate path
+        g = gpu_from([("Z" * n, 1.0)], n, thr=1e-9, capacity=1, exact=exact)
+        o = oracle_from([("Z" * n, 1.0)], n, thr=1e-9)
+        g.run(ops)
+        o.run_ops(ops)
+        (same if exact else same_set)(g, o)
+        assert len(g) > 4096
 
 
-def test_tfim_config1_every_half():
+@pytest.mark.parametrize("exact", [True, False])
+def test_tfim_config1_every_half(exact):
     wl = C.tfim_1d()
-    run_both(wl.observable, wl.n_qubits, wl.ops, thr=wl.min_abs_coeff, check_every=20)
+    run_both(wl.observable, wl.n_qubits, wl.ops, thr=wl.min_abs_coeff, check_every=20, exact=exact)
 
 
-def test_kicked_ising_prefix():
-    wl = C.kicked_ising_2d(layers=3)
+@pytest.mark.parametrize("exact", [True, False])
+def test_kicked_ising_prefix(exact):
+    wl = C.kicked_ising_2d(layers=4)
     g, o = run_both(wl.observable, wl.n_qubits, wl.ops, thr=wl.min_abs_coeff, maxw=wl.max_weight,
-                    clifford_angles=True, check_every=len(wl.ops) // 6)
-    assert len(g) > 100
+                    clifford_angles=True, check_every=len(wl.ops) // 8, exact=exact)
+    assert len(g) > 1000
 
 
 def test_kicked_ising_clifford_angle_equals_cz_sdag():
@@ -188,19 +232,21 @@ def test_kicked_ising_clifford_angle_equals_cz_sdag():
     same(g, o)
 
 
-def test_clifford_t_prefix():
+@pytest.mark.parametrize("exact", [True, False])
+def test_clifford_t_prefix(exact):
     # the term count grows ~2-4x per layer past layer 15 (6480 terms after 16 layers)
     wl = C.clifford_t(layers=16)
-    run_both(wl.observable, wl.n_qubits, wl.ops, thr=wl.min_abs_coeff, check_every=50)
+    run_both(wl.observable, wl.n_qubits, wl.ops, thr=wl.min_abs_coeff, check_every=50, exact=exact)
 
 
-def test_live_counts_match_oracle():
-    wl = C.tfim_1d(steps=3)
-    g = gpu_from(wl.observable, wl.n_qubits, wl.min_abs_coeff)
-    o = oracle_from(wl.observable, wl.n_qubits, wl.min_abs_coeff)
-    g.run(wl.ops)
-    want = o.run_ops(wl.ops, counts=True)
-    assert np.array_equal(g.live_counts(), want)
+@pytest.mark.parametrize("exact", [True, False])
+def test_live_counts_match_oracle(exact):
+    for wl in (C.tfim_1d(steps=3), C.kicked_ising_2d(layers=4)):
+        g = gpu_from(wl.observable, wl.n_qubits, wl.min_abs_coeff, wl.max_weight, wl.clifford_angles, exact=exact)
+        o = oracle_from(wl.observable, wl.n_qubits, wl.min_abs_coeff, wl.max_weight, wl.clifford_angles)
+        g.run(wl.ops)
+        want = o.run_ops(wl.ops, counts=True)
+        assert np.array_equal(g.live_counts(), want)
 
 
 def test_preserve_strings():
