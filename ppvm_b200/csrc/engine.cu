@@ -238,7 +238,8 @@ ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   CUDA_TRY(cudaMalloc(&s->table, sizeof(unsigned long long) * s->table_cap));
   CUDA_TRY(cudaMemsetAsync(s->table, 0, sizeof(unsigned long long) * s->table_cap, s->stream));
   s->table_epoch = 0;
-  s->tstate_cap = new_cap / 512 + 64;
+  // one tile-state word per look-back tile: the smallest tile is k_run_groups' kRunWarps groups
+  s->tstate_cap = new_cap / kRunWarps + 64;
   CUDA_TRY(cudaMalloc(&s->tstate, sizeof(unsigned long long) * s->tstate_cap));
   CUDA_TRY(cudaMemsetAsync(s->tstate, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
   CUDA_TRY(cudaMalloc(&s->tstate2, sizeof(unsigned long long) * s->tstate_cap));
