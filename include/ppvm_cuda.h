@@ -199,6 +199,21 @@ ppvm_status ppvm_gate_list_run(ppvm_sum* sum, const ppvm_op* ops, size_t n_ops);
  * the term-gate-updates metric); cap entries are written, n_out = n_ops of that run. */
 ppvm_status ppvm_last_run_live_counts(const ppvm_sum* sum, uint64_t* counts, size_t cap,
                                       size_t* n_out);
+/* The composed map of a list of Clifford ops (X..CY, and rotations at theta = +-pi/2 taken
+ * as the Clifford they equal), as a gate list applies it to a sum's terms: row 2q is the
+ * image of X_q, row 2q+1 the image of Z_q, as W-word X/Z planes (img_x[row*W + w],
+ * img_z[row*W + w]) and a sign (image = (-1)^sign[row] * word).  2*n_qubits rows.  Host
+ * only; no device is needed.  No per-call counterpart in the reference: the reference maps
+ * the terms gate by gate (`crates/ppvm-pauli-sum/src/sum/clifford.rs:37-221`); this is the
+ * map that ppvm_gate_list_run applies in one pass to runs of kTabMinOps (8) or more
+ * Clifford ops. */
+ppvm_status ppvm_clifford_tableau(uint32_t n_qubits, const ppvm_op* ops, size_t n_ops,
+                                  uint64_t* img_x, uint64_t* img_z, uint8_t* sign);
+/* Bytes this handle has copied host->device and device->host since it was created
+ * (terms, op and run descriptors, tableaux, control blocks, op logs, results). */
+ppvm_status ppvm_transfer_counters(const ppvm_sum* sum, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+/* Kernels this handle has launched since it was created (all families, readouts included). */
+ppvm_status ppvm_launch_count(const ppvm_sum* sum, uint64_t* out);
 
 /* ---- diagnostics ------------------------------------------------------------------- */
 /* Thread-local text of the last failing call ("" if none). */

@@ -74,6 +74,10 @@ _SIGS = {
     "ppvm_overlap": [_P, _P, _DP],
     "ppvm_gate_list_run": [_P, ctypes.POINTER(Op), _SZ],
     "ppvm_last_run_live_counts": [_P, _U64P, _SZ, _SZP],
+    "ppvm_clifford_tableau": [ctypes.c_uint32, ctypes.POINTER(Op), _SZ, _U64P, _U64P,
+                              ctypes.POINTER(ctypes.c_uint8)],
+    "ppvm_transfer_counters": [_P, _U64P, _U64P],
+    "ppvm_launch_count": [_P, _U64P],
     "ppvm_profile_enable": [_P, _I],
     "ppvm_profile_read": [_P, ctypes.c_char_p, _SZ, _DP, _U64P, _U64P, _SZ, _SZP],
 }

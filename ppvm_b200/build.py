@@ -15,9 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libppvm_cuda.so")
 SOURCES = [os.path.join(HERE, "csrc", "engine.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "kernels.cuh")] + [
-    os.path.join(ROOT, "include", "ppvm_cuda.h")
-]
+HEADERS = sorted(
+    os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc")) if f.endswith(".cuh")
+) + [os.path.join(ROOT, "include", "ppvm_cuda.h")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "-fmad=false",

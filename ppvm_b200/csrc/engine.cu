@@ -19,6 +19,7 @@
 
 #include "../../include/ppvm_cuda.h"
 #include "runs.cuh"
+#include "tableau.cuh"
 
 using namespace ppvm;
 
@@ -73,17 +74,27 @@ struct ProfLaunch {
   int family;
   int op;
   int nops;  // ops covered (Clifford runs)
+  int aux;   // fused TRUNCATE op of a tableau pass, else -1
   cudaEvent_t a, b;
 };
 
 enum Family {
   F_SCAN = 0, F_PAIR, F_APPLY, F_COMMIT, F_CLIFF, F_TRUNC, F_READ,
-  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_UNTOUCHED, F_RUN_GROUPS, F_RUN_COMMIT, F_COUNT
+  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_UNTOUCHED, F_RUN_GROUPS, F_RUN_COMMIT, F_TABLEAU, F_COUNT
 };
 const char* kFamilyNames[F_COUNT] = {"rot_scan", "rot_pair", "rot_apply", "rot_commit",
                                      "clifford", "truncate", "readout",
                                      "run_classify", "run_order", "run_scatter", "run_untouched",
-                                     "run_groups", "run_commit"};
+                                     "run_groups", "run_commit", "tableau"};
+
+// One pinned host chunk and its device twin: per-call uploads (op descriptors, run
+// descriptors, tableaux) are packed here and copied with truly asynchronous copies.
+struct StageChunk {
+  uint8_t* h = nullptr;
+  uint8_t* d = nullptr;
+  size_t cap = 0;
+  size_t used = 0;
+};
 
 }  // namespace
 
@@ -108,7 +119,6 @@ struct ppvm_sum {
   uint64_t* planes = nullptr;  // x[W*cap] z[W*cap] c[cap]
   uint64_t* alt = nullptr;     // second plane buffer: fused runs write here, then swap
   RunScratch R = {};
-  RunDesc* d_rundesc = nullptr;
   unsigned long long* tstate2 = nullptr;
   std::vector<int> swaps;      // op indices of fused runs enqueued in the current attempt
   std::set<size_t> no_fuse;    // run starts that must take the per-gate path
@@ -126,7 +136,6 @@ struct ppvm_sum {
   OpLog* h_log = nullptr;
   size_t log_cap = 0;
   size_t last_nops = 0;
-  DevOp* d_ops = nullptr;
   PatItem* d_pat = nullptr;
   double* d_partials = nullptr;
   unsigned long long* d_counter = nullptr;
@@ -139,6 +148,11 @@ struct ppvm_sum {
   unsigned tile_epoch = 0;
   unsigned table_epoch = 0;
   bool poisoned = false;
+
+  std::vector<StageChunk> stage;  // upload arena, reset at the start of every submission
+  size_t stage_cur = 0;
+  unsigned long long xfer_h2d = 0, xfer_d2h = 0;  // bytes copied host<->device since creation
+  unsigned long long launch_count = 0;            // kernels launched since creation
 
   bool prof = false;
   std::vector<ProfLaunch> prof_pending;
@@ -272,6 +286,37 @@ ppvm_status ensure_log(ppvm_sum* s, size_t nops) {
   return PPVM_OK;
 }
 
+// Copies `bytes` from src into the upload arena and enqueues its copy to the device on the
+// sum's stream; *dptr receives the device address.  The arena's contents stay valid until the
+// next stage_reset, which callers issue only after the stream has been synchronised.
+ppvm_status stage_put(ppvm_sum* s, const void* src, size_t bytes, const void** dptr) {
+  const size_t need = std::max<size_t>((bytes + 255) & ~size_t(255), 256);
+  while (s->stage_cur < s->stage.size() && s->stage[s->stage_cur].cap - s->stage[s->stage_cur].used < need)
+    ++s->stage_cur;
+  if (s->stage_cur == s->stage.size()) {
+    StageChunk ch;
+    ch.cap = std::max<size_t>(need, (size_t)1 << 20);
+    CUDA_TRY(cudaMallocHost(&ch.h, ch.cap));
+    if (cudaMalloc(&ch.d, ch.cap) != cudaSuccess) {
+      cudaFreeHost(ch.h);
+      return fail(PPVM_ECAPACITY, "device allocation of the upload arena failed");
+    }
+    s->stage.push_back(ch);
+  }
+  StageChunk& ch = s->stage[s->stage_cur];
+  std::memcpy(ch.h + ch.used, src, bytes);
+  CUDA_TRY(cudaMemcpyAsync(ch.d + ch.used, ch.h + ch.used, bytes, cudaMemcpyHostToDevice, s->stream));
+  *dptr = ch.d + ch.used;
+  ch.used += need;
+  s->xfer_h2d += bytes;
+  return PPVM_OK;
+}
+
+void stage_reset(ppvm_sum* s) {
+  for (auto& ch : s->stage) ch.used = 0;
+  s->stage_cur = 0;
+}
+
 unsigned grid_for(unsigned long long work, unsigned long long per_block, int max_per_sm) {
   unsigned long long g = (work + per_block - 1) / per_block;
   const unsigned long long cap = (unsigned long long)g_sm_count * max_per_sm;
@@ -285,11 +330,13 @@ struct ProfScope {
   ppvm_sum* s;
   ProfLaunch L;
   bool on;
-  ProfScope(ppvm_sum* sum, int family, int op, int nops) : s(sum), on(sum->prof) {
+  ProfScope(ppvm_sum* sum, int family, int op, int nops, int aux = -1) : s(sum), on(sum->prof) {
+    ++s->launch_count;
     if (!on) return;
     L.family = family;
     L.op = op;
     L.nops = nops;
+    L.aux = aux;
     L.a = take();
     L.b = take();
     cudaEventRecord(L.a, s->stream);
@@ -326,6 +373,10 @@ uint64_t launch_bytes(const ppvm_sum* s, const ProfLaunch& L, const std::vector<
     case F_TRUNC: return g.n_in * B + g.n_out * B;
     case F_RUN_CLASSIFY: return g.n_in * B;                    // every term's key read once
     case F_RUN_UNTOUCHED: return g.n_in * 8 + g.n_in * B;      // group slots + untouched terms
+    case F_TABLEAU: {  // every term read once, survivors written once
+      const uint64_t out = L.aux >= 0 ? s->h_log[L.aux].n_out : g.n_in;
+      return g.n_in * B + out * B;
+    }
     case F_RUN_GROUPS: {                                       // members read, group outputs written
       const OpLog& last = s->h_log[L.op + std::max(L.nops, 1) - 1];
       return g.n_s * B + (L.nops > 1 ? last.n_s : 0) * B;
@@ -440,6 +491,87 @@ void gen_from_op(const ppvm_sum* s, const ppvm_op& op, Gen& g) {
   (void)s;
 }
 
+// ---- Clifford tableau of a run (host) ------------------------------------------------------------
+struct HostTableau {
+  TabParams tp;
+  std::vector<uint32_t> tq;    // touched qubits, ascending (rank order)
+  std::vector<uint64_t> rows;  // per row: a[W] (X plane), b[W] (Z plane) of the image
+  std::vector<uint8_t> ph;     // image = i^ph X^a Z^b
+  std::vector<uint8_t> sign;   // image = (-1)^sign * (Hermitian word a, b)
+};
+
+bool devop_two(const DevOp& d) {
+  return d.code == C_CNOT || d.code == C_CZ || d.code == C_CY || (d.code == C_ROTC && d.two);
+}
+
+// Images of X_q and Z_q (q touched by the run) under the Clifford ops d[0..L), applied in
+// order with cliff_rule to 64 generators per word (column form: one bit per generator).
+void compose_tableau(int W, const DevOp* d, int L, HostTableau& t) {
+  std::memset(&t.tp, 0, sizeof(t.tp));
+  for (int i = 0; i < L; ++i) {
+    t.tp.T[d[i].w0] |= 1ull << d[i].b0;
+    if (devop_two(d[i])) t.tp.T[d[i].w1] |= 1ull << d[i].b1;
+  }
+  t.tq.clear();
+  std::vector<int> rank((size_t)64 * W, -1);
+  for (int w = 0; w < W; ++w) {
+    t.tp.pre[w] = (uint32_t)t.tq.size();
+    for (int b = 0; b < 64; ++b)
+      if ((t.tp.T[w] >> b) & 1ull) {
+        rank[(size_t)w * 64 + b] = (int)t.tq.size();
+        t.tq.push_back((uint32_t)(w * 64 + b));
+      }
+  }
+  const int nt = (int)t.tq.size(), R = 2 * nt, RW = (R + 63) / 64;
+  t.tp.nrows = (uint32_t)R;
+  std::vector<uint64_t> cx((size_t)nt * RW, 0), cz((size_t)nt * RW, 0), sg(RW, 0);
+  for (int r = 0; r < nt; ++r) {
+    cx[(size_t)r * RW + (2 * r) / 64] |= 1ull << ((2 * r) % 64);
+    cz[(size_t)r * RW + (2 * r + 1) / 64] |= 1ull << ((2 * r + 1) % 64);
+  }
+  for (int i = 0; i < L; ++i) {
+    const int r0 = rank[(size_t)d[i].w0 * 64 + d[i].b0];
+    const int r1 = devop_two(d[i]) ? rank[(size_t)d[i].w1 * 64 + d[i].b1] : -1;
+    for (int j = 0; j < RW; ++j) {
+      uint64_t x0 = cx[(size_t)r0 * RW + j], z0 = cz[(size_t)r0 * RW + j];
+      uint64_t x1 = r1 >= 0 ? cx[(size_t)r1 * RW + j] : 0ull, z1 = r1 >= 0 ? cz[(size_t)r1 * RW + j] : 0ull;
+      uint64_t ng = sg[j];
+      cliff_rule<uint64_t>(d[i], x0, z0, x1, z1, ng);
+      cx[(size_t)r0 * RW + j] = x0;
+      cz[(size_t)r0 * RW + j] = z0;
+      if (r1 >= 0) {
+        cx[(size_t)r1 * RW + j] = x1;
+        cz[(size_t)r1 * RW + j] = z1;
+      }
+      sg[j] = ng;
+    }
+  }
+  t.rows.assign((size_t)R * 2 * W, 0);
+  for (int c = 0; c < nt; ++c) {
+    const uint32_t q = t.tq[c];
+    for (int j = 0; j < RW; ++j) {
+      for (int pl = 0; pl < 2; ++pl) {
+        uint64_t m = (pl == 0 ? cx : cz)[(size_t)c * RW + j];
+        while (m) {
+          const int row = j * 64 + __builtin_ctzll(m);
+          m &= m - 1;
+          t.rows[(size_t)row * 2 * W + (size_t)pl * W + (q >> 6)] |= 1ull << (q & 63);
+        }
+      }
+    }
+  }
+  t.ph.assign(R, 0);
+  t.sign.assign(R, 0);
+  for (int row = 0; row < R; ++row) {
+    const uint64_t* e = &t.rows[(size_t)row * 2 * W];
+    unsigned p = 0;
+    for (int w = 0; w < W; ++w) p += (unsigned)__builtin_popcountll(e[w] & e[W + w]);
+    const bool neg = (sg[row / 64] >> (row % 64)) & 1ull;
+    t.sign[row] = neg ? 1 : 0;
+    t.ph[row] = (uint8_t)((p + (neg ? 2u : 0u)) & 3u);
+  }
+}
+
 // ---- kernel enqueue (templated on W) ------------------------------------------------------------
 template <int W>
 struct K {
@@ -506,14 +638,16 @@ struct K {
     const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
     unsigned long long tsize = next_pow2(std::max<unsigned long long>(2 * nub, 1024));
     if (tsize > s->table_cap) tsize = s->table_cap;
-    CUDA_TRY(cudaMemcpyAsync(s->d_rundesc, &rd, sizeof(RunDesc), cudaMemcpyHostToDevice, s->stream));
+    const void* d_rd_v = nullptr;
+    PPVM_TRY(stage_put(s, &rd, sizeof(RunDesc), &d_rd_v));
+    const RunDesc* d_rd = static_cast<const RunDesc*>(d_rd_v);
     CUDA_TRY(cudaMemsetAsync(s->R.grp_min, 0xFF, sizeof(uint32_t) * tsize, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->R.grp_cnt, 0, sizeof(uint32_t) * tsize, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->R.created, 0, sizeof(unsigned long long) * kRunMaxGates, s->stream));
     const int trunc = trunc_op >= 0 ? 1 : 0;
     {
       ProfScope ps(s, F_RUN_CLASSIFY, op0, L);
-      k_run_classify<W><<<grid_for(nub, 256, 8), 256, 0, s->stream>>>(P, s->d_ctrl, s->d_rundesc, s->R, s->table,
+      k_run_classify<W><<<grid_for(nub, 256, 8), 256, 0, s->stream>>>(P, s->d_ctrl, d_rd, s->R, s->table,
                                                                        tsize - 1, s->next_table_epoch(), op0);
     }
     {
@@ -534,7 +668,7 @@ struct K {
     {
       ProfScope ps(s, F_RUN_GROUPS, op0, L);
       k_run_groups<W><<<grid_for(nub, kRunWarps, 8), kRunWarps * 32, 0, s->stream>>>(
-          P, O, s->d_ctrl, s->d_rundesc, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0);
+          P, O, s->d_ctrl, d_rd, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0);
     }
     {
       ProfScope ps(s, F_RUN_COMMIT, op0, L);
@@ -547,7 +681,42 @@ struct K {
     return PPVM_OK;
   }
 
+  // A composed Clifford run ops[op0..op0+nops), optionally with its TRUNCATE (trunc_op >= 0):
+  // one pass from the planes into the alternate planes, then a swap.
+  static ppvm_status tableau(ppvm_sum* s, const HostTableau& t, int op0, int nops, int trunc_op) {
+    const Planes P = s->planes_view(), O = s->alt_view();
+    const void* d_rows = nullptr;
+    const void* d_ph = nullptr;
+    PPVM_TRY(stage_put(s, t.rows.data(), t.rows.size() * sizeof(uint64_t), &d_rows));
+    PPVM_TRY(stage_put(s, t.ph.data(), t.ph.size(), &d_ph));
+    const size_t smem = t.rows.size() * sizeof(uint64_t) + t.ph.size();
+    if (smem > kTabMaxSmem) return fail(PPVM_EINVAL, "internal: tableau exceeds shared memory");
+    static unsigned long long attr_set = 0;  // one bit per device
+    if (!((attr_set >> s->device) & 1ull)) {
+      CUDA_TRY(cudaFuncSetAttribute(k_tableau<W, kTabBlock, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kTabMaxSmem));
+      attr_set |= 1ull << s->device;
+    }
+    const int bps = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / (smem + 4096)));
+    const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
+    {
+      ProfScope ps(s, F_TABLEAU, op0, nops, trunc_op);
+      k_tableau<W, kTabBlock, ITEMS><<<grid_for(nub, (unsigned long long)kTabBlock * ITEMS, bps), kTabBlock, smem,
+                                      s->stream>>>(
+          P, O, s->d_ctrl, t.tp, static_cast<const uint64_t*>(d_rows), static_cast<const uint8_t*>(d_ph),
+          trunc_op >= 0 ? 1 : 0, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0, nops, s->d_log);
+    }
+    {
+      ProfScope ps(s, F_COMMIT, op0, nops);
+      k_commit_tableau<<<1, 1, 0, s->stream>>>(s->d_ctrl, trunc_op, s->d_log);
+    }
+    std::swap(s->planes, s->alt);
+    s->swaps.push_back(op0);
+    return PPVM_OK;
+  }
+
   static void owz(ppvm_sum* s, int nblocks) {
+    s->launch_count += 2;
     k_owz<W><<<nblocks, kRedBlock, 0, s->stream>>>(s->planes_view(), s->d_ctrl, s->d_partials);
     k_sum_partials<<<1, kRedBlock, 0, s->stream>>>(s->d_partials, nblocks, s->d_ctrl);
   }
@@ -605,6 +774,10 @@ ppvm_status enqueue_run(ppvm_sum* s, const RunDesc& rd, int op0, int L, int trun
   DISPATCH_W_RET(s->W, run(s, rd, op0, L, trunc_op));
 }
 
+ppvm_status enqueue_tableau(ppvm_sum* s, const HostTableau& t, int op0, int nops, int trunc_op) {
+  DISPATCH_W_RET(s->W, tableau(s, t, op0, nops, trunc_op));
+}
+
 int test_words_of(int W, const Gen& g) {
   int n = 0;
   for (int w = 0; w < W; ++w) n += (g.gz[w] != 0) + (g.gx[w] != 0);
@@ -615,6 +788,7 @@ int test_words_of(int W, const Gen& g) {
 ppvm_status sync_state(ppvm_sum* s, size_t nops) {
   CUDA_TRY(cudaMemcpyAsync(s->h_ctrl, s->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s->stream));
   if (nops) CUDA_TRY(cudaMemcpyAsync(s->h_log, s->d_log, sizeof(OpLog) * nops, cudaMemcpyDeviceToHost, s->stream));
+  s->xfer_d2h += sizeof(Ctrl) + sizeof(OpLog) * nops;
   CUDA_TRY(cudaStreamSynchronize(s->stream));
   return PPVM_OK;
 }
@@ -626,6 +800,7 @@ ppvm_status clear_err(ppvm_sum* s) {
   for (int t = 0; t < 4; ++t) c.tickets[t] = 0;
   CUDA_TRY(cudaMemcpyAsync(s->d_ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
+  s->xfer_h2d += sizeof(Ctrl);
   return PPVM_OK;
 }
 
@@ -633,17 +808,43 @@ ppvm_status clear_err(ppvm_sum* s) {
 // come from `gens` when ops[i].flags == 1 (index in q0).
 ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
                     const std::vector<Gen>& gens, std::vector<int>& test_words) {
-  std::vector<DevOp> run;
+  std::vector<DevOp> run;  // pending local ops (Cliffords, Clifford-angle rotations, noise)
   int run_start = -1;
-  auto flush = [&]() -> ppvm_status {
-    size_t off = 0;
-    while (off < run.size()) {
-      const int cnt = (int)std::min<size_t>(kMaxOpsPerLaunch, run.size() - off);
-      CUDA_TRY(cudaMemcpyAsync(s->d_ops, run.data() + off, sizeof(DevOp) * cnt,
-                               cudaMemcpyHostToDevice, s->stream));
-      DISPATCH_W(s->W, clifford(s, s->d_ops, cnt, run_start + (int)off));
+  // in-place per-op pass over run[a, b)
+  auto per_op = [&](size_t a, size_t b) -> ppvm_status {
+    size_t off = a;
+    while (off < b) {
+      const int cnt = (int)std::min<size_t>(kMaxOpsPerLaunch, b - off);
+      const void* d_ops = nullptr;
+      PPVM_TRY(stage_put(s, run.data() + off, sizeof(DevOp) * cnt, &d_ops));
+      DISPATCH_W(s->W, clifford(s, static_cast<const DevOp*>(d_ops), cnt, run_start + (int)off));
       off += cnt;
     }
+    return PPVM_OK;
+  };
+  // Enqueues the pending local ops.  Stretches of at least kTabMinOps Clifford ops become one
+  // tableau pass; the rest (noise ops, short stretches) take the per-op pass.  A TRUNCATE at
+  // trunc_op that directly follows the ops is fused into a final tableau pass when the sum
+  // has no preserve strings (*fused is then set).
+  auto flush = [&](int trunc_op, bool* fused) -> ppvm_status {
+    if (fused) *fused = false;
+    size_t a = 0, pend = 0;  // run[pend, a) waits for the per-op pass
+    while (a < run.size()) {
+      size_t b = a;
+      while (b < run.size() && is_cliff_code(run[b].code)) ++b;
+      if (b - a >= (size_t)kTabMinOps) {
+        PPVM_TRY(per_op(pend, a));
+        const int t_op = (b == run.size() && trunc_op >= 0 && s->npres == 0) ? trunc_op : -1;
+        HostTableau tab;
+        compose_tableau(s->W, run.data() + a, (int)(b - a), tab);
+        PPVM_TRY(enqueue_tableau(s, tab, run_start + (int)a, (int)(b - a), t_op));
+        if (t_op >= 0 && fused) *fused = true;
+        pend = a = b;
+      } else {
+        a = (b == a) ? a + 1 : b;
+      }
+    }
+    PPVM_TRY(per_op(pend, run.size()));
     run.clear();
     run_start = -1;
     return PPVM_OK;
@@ -651,7 +852,7 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
   for (size_t i = start; i < n_ops; ++i) {
     const ppvm_op& op = ops[i];
     if (op.flags == 1) {  // explicit generator
-      PPVM_TRY(flush());
+      PPVM_TRY(flush(-1, nullptr));
       const Gen& g = gens[op.q0];
       test_words[i] = test_words_of(s->W, g);
       bool cliff = is_clifford_angle(s, op.theta);
@@ -662,8 +863,9 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
       continue;
     }
     if (op.code == PPVM_OP_TRUNCATE) {
-      PPVM_TRY(flush());
-      DISPATCH_W(s->W, truncate(s, (int)i));
+      bool fused = false;
+      PPVM_TRY(flush((int)i, &fused));
+      if (!fused) DISPATCH_W(s->W, truncate(s, (int)i));
       continue;
     }
     if (is_local(s, op)) {
@@ -691,20 +893,20 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
         ++j;
       }
       if (rd.L >= 2) {
-        PPVM_TRY(flush());
+        PPVM_TRY(flush(-1, nullptr));
         const int trunc_op = (j < n_ops && ops[j].code == PPVM_OP_TRUNCATE && ops[j].flags == 0) ? (int)j : -1;
         PPVM_TRY(enqueue_run(s, rd, (int)i, (int)rd.L, trunc_op));
         i = trunc_op >= 0 ? j : j - 1;  // the loop's ++i moves past the run (and its TRUNCATE)
         continue;
       }
     }
-    PPVM_TRY(flush());
+    PPVM_TRY(flush(-1, nullptr));
     Gen g;
     gen_from_op(s, op, g);
     test_words[i] = test_words_of(s->W, g);
     DISPATCH_W(s->W, rotation(s, g, op.theta, (int)i));
   }
-  PPVM_TRY(flush());
+  PPVM_TRY(flush(-1, nullptr));
   CUDA_TRY(cudaGetLastError());
   return PPVM_OK;
 }
@@ -719,6 +921,7 @@ ppvm_status run_list(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, const std::v
   s->no_fuse.clear();
   for (int attempt = 0; attempt < 64; ++attempt) {
     s->swaps.clear();
+    stage_reset(s);  // the stream is idle here: every earlier upload has completed
     PPVM_TRY(enqueue(s, ops, n_ops, start, gens, test_words));
     PPVM_TRY(sync_state(s, n_ops));
     const Ctrl& c = *s->h_ctrl;
@@ -904,10 +1107,8 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
     return bail(fail(PPVM_ECUDA, "cudaStreamCreate failed"));
   if (cudaMalloc(&s->d_ctrl, sizeof(Ctrl)) != cudaSuccess ||
       cudaMallocHost(&s->h_ctrl, sizeof(Ctrl)) != cudaSuccess ||
-      cudaMalloc(&s->d_ops, sizeof(DevOp) * kMaxOpsPerLaunch) != cudaSuccess ||
       cudaMalloc(&s->d_partials, sizeof(double) * 8192) != cudaSuccess ||
       cudaMalloc(&s->d_counter, sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&s->d_rundesc, sizeof(RunDesc)) != cudaSuccess ||
       cudaMalloc(&s->side, sizeof(uint64_t) * (2 * s->W + 1) * (kMaxPreserve + 1)) != cudaSuccess)
     return bail(fail(PPVM_ECAPACITY, "device allocation failed"));
   std::memset(s->h_ctrl, 0, sizeof(Ctrl));
@@ -936,6 +1137,10 @@ ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
     cudaEventDestroy(L.b);
   }
   for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
+  for (auto& ch : s->stage) {
+    cudaFreeHost(ch.h);
+    cudaFree(ch.d);
+  }
   cudaFree(s->planes);
   free_scratch(s);
   cudaFree(s->side);
@@ -943,11 +1148,9 @@ ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
   cudaFreeHost(s->h_ctrl);
   cudaFree(s->d_log);
   cudaFreeHost(s->h_log);
-  cudaFree(s->d_ops);
   cudaFree(s->d_pat);
   cudaFree(s->d_partials);
   cudaFree(s->d_counter);
-  cudaFree(s->d_rundesc);
   cudaFree(s->d_pres_keys);
   cudaFree(s->d_pres_table);
   if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
@@ -1027,6 +1230,7 @@ ppvm_status ppvm_sum_add_terms(ppvm_sum* s, const uint64_t* x, const uint64_t* z
   CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(uint64_t) * W * k, cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(cudaMemcpyAsync(dz, z, sizeof(uint64_t) * W * k, cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(cudaMemcpyAsync(dc, c, sizeof(double) * k, cudaMemcpyHostToDevice, s->stream));
+  s->xfer_h2d += sizeof(uint64_t) * (2 * W + 1) * k;
   unsigned long long mask;
   unsigned ep;
   ppvm_status st = build_index(s, s->n_host + k, &mask, &ep);
@@ -1373,6 +1577,57 @@ ppvm_status ppvm_equal(const ppvm_sum* ca, const ppvm_sum* cb, int* out) {
   CUDA_TRY(cudaMemcpyAsync(&miss, a->d_counter, sizeof(miss), cudaMemcpyDeviceToHost, a->stream));
   CUDA_TRY(cudaStreamSynchronize(a->stream));
   *out = miss == 0 ? 1 : 0;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_clifford_tableau(uint32_t n_qubits, const ppvm_op* ops, size_t n_ops, uint64_t* img_x,
+                                  uint64_t* img_z, uint8_t* sign) {
+  if (n_qubits == 0 || n_qubits > 64 * kMaxW) return fail(PPVM_EINVAL, "n_qubits must be in [1, 512]");
+  if ((n_ops && !ops) || !img_x || !img_z || !sign) return fail(PPVM_EINVAL, "null argument");
+  ppvm_sum probe;  // validation only: qubit range and Clifford-angle rule
+  probe.n = n_qubits;
+  probe.flags = PPVM_FLAG_CLIFFORD_ANGLES;
+  std::vector<DevOp> d;
+  for (size_t i = 0; i < n_ops; ++i) {
+    PPVM_TRY(validate(&probe, ops[i]));
+    if (!is_local(&probe, ops[i]) || ops[i].flags != 0)
+      return fail(PPVM_EINVAL, "ppvm_clifford_tableau takes Clifford ops and rotations at +-pi/2 only");
+    d.push_back(to_devop(ops[i]));
+    if (!is_cliff_code(d.back().code)) return fail(PPVM_EINVAL, "noise channels are not Clifford maps");
+  }
+  const int W = (int)((n_qubits + 63) / 64);
+  for (uint32_t q = 0; q < n_qubits; ++q)
+    for (int p = 0; p < 2; ++p) {
+      const size_t row = 2 * (size_t)q + p;
+      for (int w = 0; w < W; ++w) img_x[row * W + w] = img_z[row * W + w] = 0;
+      (p == 0 ? img_x : img_z)[row * W + (q >> 6)] = 1ull << (q & 63);
+      sign[row] = 0;
+    }
+  if (d.empty()) return PPVM_OK;
+  HostTableau t;
+  compose_tableau(W, d.data(), (int)d.size(), t);
+  for (size_t c = 0; c < t.tq.size(); ++c)
+    for (int p = 0; p < 2; ++p) {
+      const size_t row = 2 * (size_t)t.tq[c] + p, trow = 2 * c + p;
+      for (int w = 0; w < W; ++w) {
+        img_x[row * W + w] = t.rows[trow * 2 * W + w];
+        img_z[row * W + w] = t.rows[trow * 2 * W + W + w];
+      }
+      sign[row] = t.sign[trow];
+    }
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_transfer_counters(const ppvm_sum* s, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+  if (!s || !h2d_bytes || !d2h_bytes) return fail(PPVM_EINVAL, "null argument");
+  *h2d_bytes = s->xfer_h2d;
+  *d2h_bytes = s->xfer_d2h;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_launch_count(const ppvm_sum* s, uint64_t* out) {
+  if (!s || !out) return fail(PPVM_EINVAL, "null argument");
+  *out = s->launch_count;
   return PPVM_OK;
 }
 

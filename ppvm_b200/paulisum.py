@@ -335,9 +335,22 @@ class PauliSum:
 
     # ---- gate lists ------------------------------------------------------------------------------
     def run(self, ops) -> None:
-        """Runs a gate list of ``ppvm_b200.gates`` tuples in one device submission."""
-        arr = ops_array(ops)
-        self._check(lib().ppvm_gate_list_run(self._h, arr, len(ops)))
+        """Runs a gate list (``ppvm_b200.gates`` tuples, or a ``GateList`` built once with
+        ``ops_array``) in one device submission."""
+        gl = ops if isinstance(ops, GateList) else ops_array(ops)
+        self._check(lib().ppvm_gate_list_run(self._h, gl.ptr, len(gl)))
+
+    def launch_count(self) -> int:
+        """Kernels this sum has launched since it was created."""
+        n = ctypes.c_uint64()
+        self._check(lib().ppvm_launch_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def transfer_counters(self) -> tuple[int, int]:
+        """Bytes copied host->device and device->host by this sum since it was created."""
+        h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(lib().ppvm_transfer_counters(self._h, ctypes.byref(h2d), ctypes.byref(d2h)))
+        return int(h2d.value), int(d2h.value)
 
     def live_counts(self) -> np.ndarray:
         """Live terms entering each op of the last ``run`` (term-gate-updates numerator)."""
@@ -367,13 +380,50 @@ class PauliSum:
         self._check(lib().ppvm_sum_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
 
 
-def ops_array(ops):
-    arr = (Op * max(1, len(ops)))()
-    for i, (code, q0, q1, theta, p) in enumerate(ops):
-        arr[i].code, arr[i].q0, arr[i].q1, arr[i].flags = code, q0, q1, 0
-        arr[i].theta = theta
-        arr[i].p[0], arr[i].p[1], arr[i].p[2] = p
-    return arr
+OP_DTYPE = np.dtype([("code", "<u4"), ("q0", "<u4"), ("q1", "<u4"), ("flags", "<u4"),
+                     ("theta", "<f8"), ("p", "<f8", (3,))])
+assert OP_DTYPE.itemsize == ctypes.sizeof(Op)
+
+
+class GateList:
+    """A gate list packed as ``ppvm_op`` records (numpy-backed), ready for the C ABI."""
+
+    def __init__(self, arr: np.ndarray):
+        self.arr = arr
+        self.ptr = arr.ctypes.data_as(ctypes.POINTER(Op))
+
+    def __len__(self) -> int:
+        return len(self.arr)
+
+
+def ops_array(ops) -> GateList:
+    """Packs ``(code, q0, q1, theta, (p0, p1, p2))`` tuples into ``ppvm_op`` records."""
+    arr = np.zeros(max(1, len(ops)), dtype=OP_DTYPE)
+    if ops:
+        code, q0, q1, theta, p = zip(*ops)
+        arr["code"][: len(ops)] = code
+        arr["q0"][: len(ops)] = q0
+        arr["q1"][: len(ops)] = q1
+        arr["theta"][: len(ops)] = theta
+        arr["p"][: len(ops)] = p
+    return GateList(arr[: len(ops)] if ops else arr[:0])
+
+
+def clifford_tableau(n_qubits: int, ops):
+    """Images of X_q (row 2q) and Z_q (row 2q+1) under a list of Clifford ops, as the engine
+    composes them (host only): ``(img_x[2n, W], img_z[2n, W], sign[2n])``, image =
+    (-1)^sign * word.  Rotations at +-pi/2 count as the Clifford they equal."""
+    W = G.words(n_qubits)
+    gl = ops_array(ops)
+    ix = np.zeros((2 * n_qubits, W), dtype=np.uint64)
+    iz = np.zeros((2 * n_qubits, W), dtype=np.uint64)
+    sg = np.zeros(2 * n_qubits, dtype=np.uint8)
+    st = lib().ppvm_clifford_tableau(n_qubits, gl.ptr, len(gl), _p64(ix), _p64(iz),
+                                     sg.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    if st != OK:
+        msg = lib().ppvm_last_error_string().decode(errors="replace")
+        raise ValueError(msg) if st == EINVAL else PPVMError(st, msg)
+    return ix, iz, sg
 
 
 def _p64(a):
@@ -384,4 +434,4 @@ def _pd(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-__all__ = ["PauliSum", "PPVMError", "ops_array"]
+__all__ = ["PauliSum", "PPVMError", "GateList", "ops_array", "clifford_tableau"]
