@@ -215,6 +215,47 @@ ppvm_status ppvm_transfer_counters(const ppvm_sum* sum, uint64_t* h2d_bytes, uin
 /* Kernels this handle has launched since it was created (all families, readouts included). */
 ppvm_status ppvm_launch_count(const ppvm_sum* sum, uint64_t* out);
 
+/* ---- batches of independent sums ----------------------------------------------------- */
+/* Many independent PauliSums (instances), each with its own qubit count, truncation
+ * strategy, initial terms and gate list, advanced together on one GPU: one CTA per
+ * instance, one launch per Trotter layer (a layer ends at every second TRUNCATE of an
+ * instance's list), the layer launches captured once as CUDA graphs.  Each instance's
+ * result equals a ppvm_sum run of the same list with PPVM_FLAG_EXACT_ORDER: same terms in
+ * the same order, same coefficients.  The reference runs such sets one PauliSum at a time
+ * (its benches loop over circuits, `crates/ppvm-pauli-sum/benches/trotter.rs:28-44`); there
+ * is no batch object in the reference.  Supported ops: all op codes, without explicit
+ * generators; preserve strings are not supported.  Instances have up to 512 qubits. */
+typedef struct ppvm_batch ppvm_batch; /* opaque */
+ppvm_status ppvm_batch_create(ppvm_batch** out, size_t n_inst, const uint32_t* n_qubits,
+                              const double* min_abs_coeff, const uint64_t* max_weight,
+                              uint32_t flags, int device);
+ppvm_status ppvm_batch_destroy(ppvm_batch* batch);
+ppvm_status ppvm_batch_set_stream(ppvm_batch* batch, void* cuda_stream);
+/* Initial terms of instance `inst` (ceil(n/64) words per plane), merged with += in order. */
+ppvm_status ppvm_batch_add_terms(ppvm_batch* batch, size_t inst, const uint64_t* x,
+                                 const uint64_t* z, const double* c, size_t k);
+/* Gate list of instance `inst` (as ppvm_gate_list_run takes it). */
+ppvm_status ppvm_batch_set_ops(ppvm_batch* batch, size_t inst, const ppvm_op* ops, size_t n_ops);
+/* Runs every instance from its initial terms through its whole list (layer graphs). */
+ppvm_status ppvm_batch_run(ppvm_batch* batch);
+/* The same in one launch: each CTA runs its instance's whole list. */
+ppvm_status ppvm_batch_run_persistent(ppvm_batch* batch);
+/* Launch configuration: CTA size (128, 256, 512), items per thread (2, 4) and pair-table
+ * slots per term of capacity (2, 4).  ppvm_batch_autotune times every combination on this
+ * batch (a full run each) and keeps the fastest; best_ms = its run time. */
+ppvm_status ppvm_batch_set_config(ppvm_batch* batch, int block, int items, int table_factor);
+ppvm_status ppvm_batch_get_config(const ppvm_batch* batch, int* block, int* items, int* table_factor);
+ppvm_status ppvm_batch_autotune(ppvm_batch* batch, int* block, int* items, int* table_factor,
+                                double* best_ms);
+/* Readouts after a run: overlap_with_zero of every instance (n_inst doubles), live terms,
+ * terms of one instance (its own word count per plane), term-gate updates (per instance
+ * and total; NULL skips either). */
+ppvm_status ppvm_batch_overlap_with_zero(ppvm_batch* batch, double* out);
+ppvm_status ppvm_batch_len(const ppvm_batch* batch, size_t inst, size_t* out);
+ppvm_status ppvm_batch_export_terms(ppvm_batch* batch, size_t inst, uint64_t* x, uint64_t* z,
+                                    double* c, size_t cap, size_t* n_out);
+ppvm_status ppvm_batch_term_gate_updates(const ppvm_batch* batch, uint64_t* per_inst, uint64_t* total);
+
 /* ---- diagnostics ------------------------------------------------------------------- */
 /* Thread-local text of the last failing call ("" if none). */
 const char* ppvm_last_error_string(void);

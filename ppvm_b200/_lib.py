@@ -78,6 +78,20 @@ _SIGS = {
                               ctypes.POINTER(ctypes.c_uint8)],
     "ppvm_transfer_counters": [_P, _U64P, _U64P],
     "ppvm_launch_count": [_P, _U64P],
+    "ppvm_batch_create": [ctypes.POINTER(_P), _SZ, _U32P, _DP, _U64P, ctypes.c_uint32, _I],
+    "ppvm_batch_destroy": [_P],
+    "ppvm_batch_set_stream": [_P, _P],
+    "ppvm_batch_add_terms": [_P, _SZ, _U64P, _U64P, _DP, _SZ],
+    "ppvm_batch_set_ops": [_P, _SZ, ctypes.POINTER(Op), _SZ],
+    "ppvm_batch_run": [_P],
+    "ppvm_batch_run_persistent": [_P],
+    "ppvm_batch_set_config": [_P, _I, _I, _I],
+    "ppvm_batch_get_config": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "ppvm_batch_autotune": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), _DP],
+    "ppvm_batch_overlap_with_zero": [_P, _DP],
+    "ppvm_batch_len": [_P, _SZ, _SZP],
+    "ppvm_batch_export_terms": [_P, _SZ, _U64P, _U64P, _DP, _SZ, _SZP],
+    "ppvm_batch_term_gate_updates": [_P, _U64P, _U64P],
     "ppvm_profile_enable": [_P, _I],
     "ppvm_profile_read": [_P, ctypes.c_char_p, _SZ, _DP, _U64P, _U64P, _SZ, _SZP],
 }

@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libppvm_cuda.so")
-SOURCES = [os.path.join(HERE, "csrc", "engine.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "batch.cu", "noalloc.cu")]
 HEADERS = sorted(
     os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc")) if f.endswith(".cuh")
 ) + [os.path.join(ROOT, "include", "ppvm_cuda.h")]
@@ -39,16 +39,35 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
+    """Compiles every source to an object (in parallel), then links the shared library."""
     if not force and not stale():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", LIB, *SOURCES]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        objs.append(obj)
+        cmd = [nvcc(), *compile_flags, *extra, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    errors = []
+    for cmd, p in procs:
+        out, err = p.communicate()
+        if p.returncode != 0:
+            errors.append(f"{' '.join(cmd)}\n{out}\n{err}")
+        elif verbose and err:
+            print(err, file=sys.stderr)
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
+            "-o", LIB, *objs]
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed:\n{r.stdout}\n{r.stderr}")
-    if verbose and r.stderr:
-        print(r.stderr, file=sys.stderr)
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

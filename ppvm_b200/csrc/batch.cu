@@ -1,0 +1,1154 @@
+// batch.cu — many independent PauliSums advanced together: one CTA per sum.
+//
+// A batch holds K sums (instances) of up to 64*W qubits, each with its own gate list,
+// truncation strategy and term capacity.  All instances live in one device pool; an
+// instance table gives each one its region (offset table).  k_batch runs one Trotter layer
+// of every instance per launch (a layer ends at every second TRUNCATE of the instance's
+// list): CTA b interprets instance b's ops in order, entirely inside the CTA, so the only
+// synchronisation is __syncthreads.  The layer launches are captured once as CUDA graphs
+// and replayed.
+//
+// Per op, with reference semantics (crates/ppvm-pauli-sum/src/sum/data.rs:204-311):
+//   rotation   scan (anticommuting terms, in order) -> pair (partner K^G through an
+//              epoch-tagged table) -> apply (parent c*cos + partner's c*(eps*sin); the
+//              partnerless append their child c*(eps*sin) at the end, in parent order)
+//   Clifford / noise   in place, consecutive ops fused per term
+//   TRUNCATE   stable in-place compaction (|c| < thr or weight > cap dropped)
+// Term order therefore stays the reference's IndexMap order, and every coefficient is the
+// same IEEE result, so each instance equals a PauliSum run on its own.  A rotation that
+// would overflow its instance's capacity stops before writing anything; the host grows that
+// instance's region and resumes from the failing op.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ppvm_cuda.h"
+#include "tableau.cuh"
+
+namespace ppvm {
+void set_last_error(const std::string& msg);
+}
+
+using namespace ppvm;
+
+namespace {
+
+enum BKind : uint32_t { B_ROT = 0, B_LOCAL = 1, B_TRUNC = 2 };
+
+struct BOp {
+  uint32_t kind;
+  uint32_t pad;
+  double sn, cs;  // rotation: sin, cos of theta (host libm, as the reference's f64::sin_cos)
+  DevOp d;        // qubits; rotation axes in ax/az/two; local ops as the per-op pass encodes them
+};
+
+struct BInst {
+  unsigned long long off;    // region offset in the pool (u64 words)
+  unsigned long long cap;    // term capacity of the region
+  unsigned long long n;      // live terms
+  unsigned long long tsize;  // pair-table slots (power of two)
+  unsigned long long tgu;    // term-gate updates so far
+  unsigned long long need;   // terms needed at a failing op
+  double thr;
+  unsigned long long maxw;
+  uint32_t op_begin, op_end, pc, layer_off, n_layers, epoch;
+  int err;
+  int pad;
+};
+
+constexpr unsigned kBNone = 0xFFFFFFFFu;
+
+unsigned long long region_words(int W, unsigned long long cap, unsigned long long tsize) {
+  return (unsigned long long)(2 * W + 3) * cap + tsize;
+}
+
+template <int W>
+struct Region {
+  uint64_t* x;
+  uint64_t* z;
+  double* c;
+  double* rc;      // coefficients of the anticommuting terms, before the op
+  uint32_t* sidx;  // index of anticommuting term r
+  uint32_t* part;  // its partner record, or kBNone
+  unsigned long long* table;
+  unsigned long long cap, tsize;
+};
+
+template <int W>
+__device__ __forceinline__ Region<W> region_of(uint64_t* pool, const BInst& I) {
+  Region<W> r;
+  uint64_t* b = pool + I.off;
+  const unsigned long long cap = I.cap;
+  r.cap = cap;
+  r.tsize = I.tsize;
+  r.x = b;
+  r.z = b + (size_t)W * cap;
+  r.c = reinterpret_cast<double*>(b + (size_t)2 * W * cap);
+  r.rc = reinterpret_cast<double*>(b + (size_t)(2 * W + 1) * cap);
+  r.sidx = reinterpret_cast<uint32_t*>(b + (size_t)(2 * W + 2) * cap);
+  r.part = r.sidx + cap;
+  r.table = reinterpret_cast<unsigned long long*>(b + (size_t)(2 * W + 3) * cap);
+  return r;
+}
+
+template <int W>
+__device__ __forceinline__ void rload(const Region<W>& R, unsigned long long i, uint64_t (&x)[W], uint64_t (&z)[W]) {
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    x[w] = R.x[(size_t)w * R.cap + i];
+    z[w] = R.z[(size_t)w * R.cap + i];
+  }
+}
+template <int W>
+__device__ __forceinline__ void rstore(const Region<W>& R, unsigned long long i, const uint64_t (&x)[W],
+                                       const uint64_t (&z)[W]) {
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    R.x[(size_t)w * R.cap + i] = x[w];
+    R.z[(size_t)w * R.cap + i] = z[w];
+  }
+}
+// word w of a W-word array without dynamic register indexing
+template <int W>
+__device__ __forceinline__ uint64_t wsel(const uint64_t (&a)[W], unsigned w) {
+  uint64_t v = 0;
+#pragma unroll
+  for (int k = 0; k < W; ++k) v = (k == (int)w) ? a[k] : v;
+  return v;
+}
+template <int W>
+__device__ __forceinline__ void wflip(uint64_t (&a)[W], unsigned w, uint64_t m) {
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    if (k == (int)w) a[k] ^= m;
+}
+template <int W>
+__device__ __forceinline__ void wset(uint64_t (&a)[W], unsigned w, unsigned b, bool v) {
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    if (k == (int)w) a[k] = (a[k] & ~(1ull << b)) | ((uint64_t)v << b);
+}
+
+// Rotation on at most two qubits with axes (ax, az) (bit 0: q0, bit 1: q1).  For a word with
+// bits (x0, z0) at q0 and (x1, z1) at q1: whether it anticommutes, and eps of its child
+// (+1 exactly when the anticommuting qubit's single-qubit phase in G*P is -1, as rot_sign).
+struct RotBits {
+  bool anti;
+  bool eps_plus;
+};
+__device__ __forceinline__ RotBits rot_bits(const DevOp& d, bool x0, bool z0, bool x1, bool z1) {
+  const bool ax0 = d.ax & 1, az0 = d.az & 1, ax1 = d.two && (d.ax & 2), az1 = d.two && (d.az & 2);
+  RotBits r;
+  r.anti = ((x0 & az0) ^ (z0 & ax0)) ^ ((x1 & az1) ^ (z1 & ax1));
+  const bool m0 = (ax0 & !az0 & !x0 & z0) | (ax0 & az0 & x0 & !z0) | (!ax0 & az0 & x0 & z0);
+  const bool m1 = (ax1 & !az1 & !x1 & z1) | (ax1 & az1 & x1 & !z1) | (!ax1 & az1 & x1 & z1);
+  r.eps_plus = m0 | m1;
+  return r;
+}
+
+template <int W>
+__device__ __forceinline__ void op_bits(const DevOp& d, const uint64_t (&x)[W], const uint64_t (&z)[W], bool& x0,
+                                        bool& z0, bool& x1, bool& z1) {
+  x0 = (wsel<W>(x, d.w0) >> d.b0) & 1ull;
+  z0 = (wsel<W>(z, d.w0) >> d.b0) & 1ull;
+  x1 = (wsel<W>(x, d.w1) >> d.b1) & 1ull;
+  z1 = (wsel<W>(z, d.w1) >> d.b1) & 1ull;
+}
+
+template <int W>
+__device__ __forceinline__ void flip_gen(const DevOp& d, uint64_t (&x)[W], uint64_t (&z)[W]) {
+  if (d.ax & 1) wflip<W>(x, d.w0, 1ull << d.b0);
+  if (d.az & 1) wflip<W>(z, d.w0, 1ull << d.b0);
+  if (d.two) {
+    if (d.ax & 2) wflip<W>(x, d.w1, 1ull << d.b1);
+    if (d.az & 2) wflip<W>(z, d.w1, 1ull << d.b1);
+  }
+}
+
+// Bits of term i at the op's qubits, read from the planes (two words at most).
+template <int W>
+__device__ __forceinline__ void term_bits(const Region<W>& R, const DevOp& d, unsigned long long i, bool& x0,
+                                          bool& z0, bool& x1, bool& z1) {
+  x0 = (R.x[(size_t)d.w0 * R.cap + i] >> d.b0) & 1ull;
+  z0 = (R.z[(size_t)d.w0 * R.cap + i] >> d.b0) & 1ull;
+  x1 = z1 = false;
+  if (d.two) {
+    x1 = (R.x[(size_t)d.w1 * R.cap + i] >> d.b1) & 1ull;
+    z1 = (R.z[(size_t)d.w1 * R.cap + i] >> d.b1) & 1ull;
+  }
+}
+
+// One local op (Clifford, Clifford-angle rotation or diagonal noise) on a word, the rules of
+// the per-op pass (crates/ppvm-pauli-sum/src/sum/clifford.rs:37-221, sum/noise.rs:17-129).
+template <int W>
+__device__ __forceinline__ void local_op(const DevOp& d, uint64_t (&x)[W], uint64_t (&z)[W], double& c, bool& neg) {
+  bool x0, z0, x1, z1;
+  op_bits<W>(d, x, z, x0, z0, x1, z1);
+  switch (d.code) {
+    case C_PAULI_ERROR: {
+      const int k = (int)x0 | ((int)z0 << 1);
+      if (k == 1) c = __dmul_rn(c, d.f0);
+      else if (k == 2) c = __dmul_rn(c, d.f1);
+      else if (k == 3) c = __dmul_rn(c, d.f2);
+      return;
+    }
+    case C_DEP1:
+      if (x0 | z0) c = __dmul_rn(c, d.f0);
+      return;
+    case C_DEP2:
+      if (x0 | z0 | x1 | z1) c = __dmul_rn(c, d.f0);
+      return;
+    default: break;
+  }
+  const bool two = d.code == C_CNOT || d.code == C_CZ || d.code == C_CY || (d.code == C_ROTC && d.two);
+  if (!two) x1 = z1 = false;
+  cliff_rule<bool>(d, x0, z0, x1, z1, neg);
+  wset<W>(x, d.w0, d.b0, x0);
+  wset<W>(z, d.w0, d.b0, z0);
+  if (two) {
+    wset<W>(x, d.w1, d.b1, x1);
+    wset<W>(z, d.w1, d.b1, z1);
+  }
+}
+
+template <int BLOCK>
+__device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v, unsigned long long* s_red) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_red[warp] = v;
+  __syncthreads();
+  unsigned long long t = 0;
+#pragma unroll
+  for (int w = 0; w < BLOCK / 32; ++w) t += s_red[w];
+  __syncthreads();
+  return t;
+}
+
+// One layer (or, with layer < 0, everything left) of every instance; CTA b = instance b.
+template <int W, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK)
+k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ layer_ends, int layer,
+        uint64_t* pool) {
+  constexpr int NW = BLOCK / 32;
+  constexpr unsigned long long TILE = (unsigned long long)BLOCK * ITEMS;
+  __shared__ unsigned s_base[ITEMS * NW + 1];
+  __shared__ unsigned long long s_red[NW];
+  BInst& I = insts[blockIdx.x];
+  if (I.err) return;
+  const unsigned end = (layer < 0 || (unsigned)layer >= I.n_layers)
+                           ? I.op_end
+                           : min(I.op_end, layer_ends[I.layer_off + (unsigned)layer]);
+  unsigned pc = I.pc;
+  if (pc >= end) return;
+  const Region<W> R = region_of<W>(pool, I);
+  const double thr = I.thr;
+  const unsigned long long maxw = I.maxw;
+  const bool wcap = maxw != ~0ull;
+  unsigned long long N = I.n, tgu = 0;
+  unsigned epoch = I.epoch;
+  int err = 0;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  while (pc < end) {
+    const uint32_t kind = ops[pc].kind;
+    if (kind == B_TRUNC) {
+      // stable in-place compaction: a tile's reads finish (inside tile_ranks) before its
+      // writes, and every write goes to a position at or below the word it came from
+      unsigned long long kept = 0;
+      for (unsigned long long base = 0; base < N; base += TILE) {
+        uint64_t kx[ITEMS][W], kz[ITEMS][W];
+        double kc[ITEMS];
+        unsigned bal[ITEMS];
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+          const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
+          bool keep = false;
+          if (i < N) {
+            rload<W>(R, i, kx[k], kz[k]);
+            kc[k] = R.c[i];
+            keep = !(fabs(kc[k]) < thr);
+            if (wcap) keep = keep && (weight<W>(kx[k], kz[k]) <= maxw);
+          }
+          bal[k] = __ballot_sync(kFull, keep);
+        }
+        const unsigned agg = tile_ranks<BLOCK, ITEMS>(bal, s_base);
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k)
+          if ((bal[k] >> lane) & 1u) {
+            const unsigned long long r = kept + s_base[k * NW + warp] + __popc(bal[k] & lt);
+            rstore<W>(R, r, kx[k], kz[k]);
+            R.c[r] = kc[k];
+          }
+        kept += agg;
+        __syncthreads();
+      }
+      N = kept;
+      ++pc;
+      continue;
+    }
+    if (kind == B_LOCAL) {
+      unsigned j = pc;
+      while (j < end && ops[j].kind == B_LOCAL) ++j;
+      for (unsigned long long i = threadIdx.x; i < N; i += BLOCK) {
+        uint64_t x[W], z[W];
+        rload<W>(R, i, x, z);
+        double c = R.c[i];
+        bool neg = false;
+        for (unsigned o = pc; o < j; ++o) local_op<W>(ops[o].d, x, z, c, neg);
+        rstore<W>(R, i, x, z);
+        R.c[i] = neg ? -c : c;
+      }
+      tgu += N * (unsigned long long)(j - pc);
+      pc = j;
+      __syncthreads();
+      continue;
+    }
+    // ---- rotation exp(-i theta/2 G), G on op.d's one or two qubits ----
+    const DevOp d = ops[pc].d;
+    const double sn = ops[pc].sn, cs = ops[pc].cs;
+    if (++epoch >= 0xFFFFu) {  // pair-table epochs wrapped: clear the table once
+      for (unsigned long long t = threadIdx.x; t < R.tsize; t += BLOCK) R.table[t] = 0ull;
+      __syncthreads();
+      epoch = 1;
+    }
+    // scan: anticommuting terms, in order
+    unsigned long long S = 0;
+    for (unsigned long long base = 0; base < N; base += TILE) {
+      unsigned bal[ITEMS];
+#pragma unroll
+      for (int k = 0; k < ITEMS; ++k) {
+        const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
+        bool a = false;
+        if (i < N) {
+          bool x0, z0, x1, z1;
+          term_bits<W>(R, d, i, x0, z0, x1, z1);
+          a = rot_bits(d, x0, z0, x1, z1).anti;
+        }
+        bal[k] = __ballot_sync(kFull, a);
+      }
+      const unsigned agg = tile_ranks<BLOCK, ITEMS>(bal, s_base);
+#pragma unroll
+      for (int k = 0; k < ITEMS; ++k)
+        if ((bal[k] >> lane) & 1u) {
+          const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
+          const unsigned long long r = S + s_base[k * NW + warp] + __popc(bal[k] & lt);
+          R.sidx[r] = (uint32_t)i;
+          R.part[r] = kBNone;
+          R.rc[r] = R.c[i];
+        }
+      S += agg;
+      __syncthreads();
+    }
+    // pair: the record of K and the record of K^G (if both exist) meet at min(K, K^G)
+    unsigned long long mine = 0;
+    const unsigned long long mask = R.tsize - 1;
+    for (unsigned long long r = threadIdx.x; r < S; r += BLOCK) {
+      uint64_t x[W], z[W], px[W], pz[W];
+      rload<W>(R, R.sidx[r], x, z);
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        px[w] = x[w];
+        pz[w] = z[w];
+      }
+      flip_gen<W>(d, px, pz);
+      const bool use_p = key_less<W>(px, pz, x, z);
+      uint64_t kx[W], kz[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        kx[w] = use_p ? px[w] : x[w];
+        kz[w] = use_p ? pz[w] : z[w];
+      }
+      const uint64_t h = hash_key<W>(kx, kz);
+      const unsigned tag = (unsigned)(h >> 48) & 0xFFFFu;
+      const unsigned long long me = make_slot(epoch, tag, (unsigned)r);
+      unsigned long long slot = h & mask, probes = 0;
+      while (true) {
+        const unsigned long long cur = ld_volatile(&R.table[slot]);
+        if (slot_epoch(cur) != (epoch & 0xFFFFu)) {
+          if (atomicCAS(&R.table[slot], cur, me) == cur) break;
+          continue;
+        }
+        if (slot_tag(cur) == tag) {
+          const unsigned j = slot_idx(cur);
+          uint64_t jx[W], jz[W];
+          rload<W>(R, R.sidx[j], jx, jz);
+          bool eq = true;
+#pragma unroll
+          for (int w = 0; w < W; ++w) eq &= (jx[w] == px[w]) & (jz[w] == pz[w]);
+          if (eq) {
+            R.part[r] = j;
+            R.part[j] = (uint32_t)r;
+            ++mine;
+            break;
+          }
+        }
+        slot = (slot + 1) & mask;
+        if (++probes > mask) {
+          err = kErrProbe;  // cannot happen with tsize >= 2 * cap; reported, not trapped
+          break;
+        }
+      }
+    }
+    const unsigned long long pairs = block_sum_u64<BLOCK>(mine, s_red);
+    const unsigned long long perr = block_sum_u64<BLOCK>((unsigned long long)err, s_red);
+    if (perr) {
+      err = kErrProbe;
+      break;
+    }
+    const unsigned long long children = S - 2 * pairs;
+    if (N + children > R.cap) {
+      if (threadIdx.x == 0) I.need = N + children;
+      err = kErrCapacity;
+      break;
+    }
+    // apply: parents in place, partnerless children appended in parent order
+    unsigned long long C = 0;
+    for (unsigned long long base = 0; base < S; base += TILE) {
+      unsigned bal[ITEMS];
+#pragma unroll
+      for (int k = 0; k < ITEMS; ++k) {
+        const unsigned long long r = base + (unsigned long long)k * BLOCK + threadIdx.x;
+        bool child = false;
+        if (r < S) {
+          const uint32_t i = R.sidx[r], j = R.part[r];
+          const double c = R.rc[r];
+          double nc;
+          if (j != kBNone) {
+            // the partner's key is K^G: its eps from this term's bits with G's bits flipped
+            bool x0, z0, x1, z1;
+            term_bits<W>(R, d, i, x0, z0, x1, z1);
+            x0 ^= (bool)(d.ax & 1);
+            z0 ^= (bool)(d.az & 1);
+            if (d.two) {
+              x1 ^= (bool)(d.ax & 2);
+              z1 ^= (bool)(d.az & 2);
+            }
+            const double eps_j = rot_bits(d, x0, z0, x1, z1).eps_plus ? 1.0 : -1.0;
+            nc = __dadd_rn(__dmul_rn(c, cs), __dmul_rn(R.rc[j], eps_j * sn));
+          } else {
+            nc = __dmul_rn(c, cs);
+            child = true;
+          }
+          R.c[i] = nc;
+        }
+        bal[k] = __ballot_sync(kFull, child);
+      }
+      const unsigned agg = tile_ranks<BLOCK, ITEMS>(bal, s_base);
+#pragma unroll
+      for (int k = 0; k < ITEMS; ++k)
+        if ((bal[k] >> lane) & 1u) {
+          const unsigned long long r = base + (unsigned long long)k * BLOCK + threadIdx.x;
+          const unsigned long long pos = N + C + s_base[k * NW + warp] + __popc(bal[k] & lt);
+          uint64_t x[W], z[W];
+          rload<W>(R, R.sidx[r], x, z);
+          bool x0, z0, x1, z1;
+          op_bits<W>(d, x, z, x0, z0, x1, z1);
+          if (!d.two) x1 = z1 = false;
+          const double eps = rot_bits(d, x0, z0, x1, z1).eps_plus ? 1.0 : -1.0;
+          flip_gen<W>(d, x, z);
+          rstore<W>(R, pos, x, z);
+          R.c[pos] = __dmul_rn(R.rc[r], eps * sn);
+        }
+      C += agg;
+      __syncthreads();
+    }
+    tgu += N;
+    N += C;
+    ++pc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    I.n = N;
+    I.pc = pc;
+    I.tgu += tgu;
+    I.epoch = epoch;
+    if (err) I.err = err;
+  }
+}
+
+// overlap_with_zero of every instance: CTA b sums instance b's coefficients of words
+// without X bits, in a fixed order (thread-strided partial sums, then a fixed tree).
+template <int W>
+__global__ void __launch_bounds__(256) k_batch_owz(const BInst* insts, uint64_t* pool, double* out) {
+  __shared__ double s_red[8];
+  const BInst& I = insts[blockIdx.x];
+  const Region<W> R = region_of<W>(pool, I);
+  double acc = 0.0;
+  for (unsigned long long i = threadIdx.x; i < I.n; i += blockDim.x) {
+    uint64_t any = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) any |= R.x[(size_t)w * R.cap + i];
+    if (any == 0) acc = __dadd_rn(acc, R.c[i]);
+  }
+  const double b = block_sum(acc, s_red);
+  if (threadIdx.x == 0) out[blockIdx.x] = b;
+}
+
+// Loads initial terms (packed per instance: x[k][W], z[k][W], c[k] at src_off) into regions.
+template <int W>
+__global__ void k_batch_load(const BInst* insts, const unsigned long long* src_off, const uint64_t* src,
+                             uint64_t* pool) {
+  const BInst& I = insts[blockIdx.x];
+  const Region<W> R = region_of<W>(pool, I);
+  const uint64_t* s = src + src_off[blockIdx.x];
+  const unsigned long long k = I.n;
+  for (unsigned long long i = threadIdx.x; i < k; i += blockDim.x) {
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      R.x[(size_t)w * R.cap + i] = s[i * W + w];
+      R.z[(size_t)w * R.cap + i] = s[k * W + i * W + w];
+    }
+    R.c[i] = __longlong_as_double((long long)s[2 * k * W + i]);
+  }
+}
+
+// Moves every instance's live terms from the old layout to the new one (capacity growth).
+template <int W>
+__global__ void k_batch_relocate(const BInst* old_i, const BInst* new_i, uint64_t* old_pool, uint64_t* new_pool) {
+  const Region<W> A = region_of<W>(old_pool, old_i[blockIdx.x]);
+  const Region<W> B = region_of<W>(new_pool, new_i[blockIdx.x]);
+  const unsigned long long n = old_i[blockIdx.x].n;
+  for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) {
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      B.x[(size_t)w * B.cap + i] = A.x[(size_t)w * A.cap + i];
+      B.z[(size_t)w * B.cap + i] = A.z[(size_t)w * A.cap + i];
+    }
+    B.c[i] = A.c[i];
+  }
+}
+
+ppvm_status bfail(ppvm_status s, const std::string& msg) {
+  ppvm::set_last_error(msg);
+  return s;
+}
+
+#define BCUDA(expr)                                                                          \
+  do {                                                                                       \
+    cudaError_t e_ = (expr);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return bfail(e_ == cudaErrorMemoryAllocation ? PPVM_ECAPACITY : PPVM_ECUDA,            \
+                   std::string(#expr) + ": " + cudaGetErrorString(e_));                      \
+  } while (0)
+
+#define BTRY(expr)                \
+  do {                            \
+    ppvm_status s_ = (expr);      \
+    if (s_ != PPVM_OK) return s_; \
+  } while (0)
+
+unsigned long long pow2_at_least(unsigned long long v) {
+  unsigned long long p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+}  // namespace
+
+struct ppvm_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  int W = 1;
+  uint32_t flags = 0;
+  size_t ninst = 0;
+  std::vector<uint32_t> nq;
+  std::vector<double> thr;
+  std::vector<uint64_t> maxw;
+  // initial terms per instance (instance words: ceil(n/64) per plane)
+  std::vector<std::vector<uint64_t>> ix, iz;
+  std::vector<std::vector<double>> ic;
+  std::vector<std::vector<BOp>> ops;
+  std::vector<std::vector<uint32_t>> lends;  // op index just past each layer's closing TRUNCATE
+  std::vector<unsigned long long> cap;       // region capacities (kept across runs)
+  // launch configuration (autotuned)
+  int block = 256, items = 4, tfac = 2;
+  // device state
+  BInst* d_inst = nullptr;
+  BInst* h_inst = nullptr;  // pinned mirror
+  BOp* d_ops = nullptr;
+  uint32_t* d_lends = nullptr;
+  uint64_t* pool = nullptr;
+  size_t pool_words = 0;
+  double* d_out = nullptr;
+  bool ops_dirty = true;
+  bool layout_dirty = true;
+  std::vector<cudaGraphExec_t> graphs;
+  int graph_cfg[3] = {0, 0, 0};
+  uint32_t max_layers = 0;
+  bool ran = false;
+};
+
+namespace {
+
+void drop_graphs(ppvm_batch* b) {
+  for (auto g : b->graphs)
+    if (g) cudaGraphExecDestroy(g);
+  b->graphs.clear();
+}
+
+int words_of(uint32_t n) { return (int)((n + 63) / 64); }
+
+// Batch plane width: 1, 2, 4 or 8 words.
+int batch_words(uint32_t n_max) {
+  const int w = words_of(n_max);
+  return w <= 1 ? 1 : w <= 2 ? 2 : w <= 4 ? 4 : 8;
+}
+
+template <int W, int BLOCK, int ITEMS>
+cudaError_t launch_layer(ppvm_batch* b, int layer) {
+  k_batch<W, BLOCK, ITEMS><<<(unsigned)b->ninst, BLOCK, 0, b->stream>>>(b->d_inst, b->d_ops, b->d_lends, layer,
+                                                                         b->pool);
+  return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t launch_layer_w(ppvm_batch* b, int layer) {
+  const int k = (b->block == 128 ? 0 : b->block == 256 ? 1 : 2) * 2 + (b->items == 2 ? 0 : 1);
+  switch (k) {
+    case 0: return launch_layer<W, 128, 2>(b, layer);
+    case 1: return launch_layer<W, 128, 4>(b, layer);
+    case 2: return launch_layer<W, 256, 2>(b, layer);
+    case 3: return launch_layer<W, 256, 4>(b, layer);
+    case 4: return launch_layer<W, 512, 2>(b, layer);
+    default: return launch_layer<W, 512, 4>(b, layer);
+  }
+}
+
+cudaError_t launch_any(ppvm_batch* b, int layer) {
+  switch (b->W) {
+    case 1: return launch_layer_w<1>(b, layer);
+    case 2: return launch_layer_w<2>(b, layer);
+    case 4: return launch_layer_w<4>(b, layer);
+    default: return launch_layer_w<8>(b, layer);
+  }
+}
+
+template <int W>
+void launch_relocate(ppvm_batch* b, const BInst* d_old, uint64_t* old_pool, uint64_t* new_pool) {
+  k_batch_relocate<W><<<(unsigned)b->ninst, 256, 0, b->stream>>>(d_old, b->d_inst, old_pool, new_pool);
+}
+template <int W>
+void launch_load(ppvm_batch* b, const unsigned long long* d_off, const uint64_t* d_src) {
+  k_batch_load<W><<<(unsigned)b->ninst, 256, 0, b->stream>>>(b->d_inst, d_off, d_src, b->pool);
+}
+template <int W>
+void launch_owz(ppvm_batch* b) {
+  k_batch_owz<W><<<(unsigned)b->ninst, 256, 0, b->stream>>>(b->d_inst, b->pool, b->d_out);
+}
+#define BDISPATCH(W_, FN, ...)          \
+  switch (W_) {                         \
+    case 1: FN<1>(__VA_ARGS__); break;  \
+    case 2: FN<2>(__VA_ARGS__); break;  \
+    case 4: FN<4>(__VA_ARGS__); break;  \
+    default: FN<8>(__VA_ARGS__); break; \
+  }
+
+ppvm_status upload_ops(ppvm_batch* b) {
+  if (!b->ops_dirty) return PPVM_OK;
+  std::vector<BOp> all;
+  std::vector<uint32_t> le;
+  b->max_layers = 0;
+  for (size_t i = 0; i < b->ninst; ++i) {
+    BInst& I = b->h_inst[i];
+    I.op_begin = (uint32_t)all.size();
+    I.layer_off = (uint32_t)le.size();
+    for (uint32_t e : b->lends[i]) le.push_back(I.op_begin + e);
+    I.n_layers = (uint32_t)b->lends[i].size();
+    all.insert(all.end(), b->ops[i].begin(), b->ops[i].end());
+    I.op_end = (uint32_t)all.size();
+    b->max_layers = std::max(b->max_layers, I.n_layers);
+  }
+  if (all.size() >= 0xFFFFFFF0ull) return bfail(PPVM_ECAPACITY, "batch op list too long");
+  cudaFree(b->d_ops);
+  cudaFree(b->d_lends);
+  b->d_ops = nullptr;
+  b->d_lends = nullptr;
+  BCUDA(cudaMalloc(&b->d_ops, sizeof(BOp) * std::max<size_t>(all.size(), 1)));
+  BCUDA(cudaMalloc(&b->d_lends, sizeof(uint32_t) * std::max<size_t>(le.size(), 1)));
+  if (!all.empty())
+    BCUDA(cudaMemcpyAsync(b->d_ops, all.data(), sizeof(BOp) * all.size(), cudaMemcpyHostToDevice, b->stream));
+  if (!le.empty())
+    BCUDA(cudaMemcpyAsync(b->d_lends, le.data(), sizeof(uint32_t) * le.size(), cudaMemcpyHostToDevice, b->stream));
+  BCUDA(cudaStreamSynchronize(b->stream));
+  b->ops_dirty = false;
+  drop_graphs(b);
+  return PPVM_OK;
+}
+
+// Lays the pool out for the current capacities.  With keep, live terms move over.
+ppvm_status layout(ppvm_batch* b, bool keep) {
+  std::vector<BInst> old(b->h_inst, b->h_inst + b->ninst);
+  unsigned long long words = 0;
+  for (size_t i = 0; i < b->ninst; ++i) {
+    BInst& I = b->h_inst[i];
+    I.cap = b->cap[i];
+    I.tsize = pow2_at_least(std::max<unsigned long long>((unsigned long long)b->tfac * I.cap, 64));
+    I.off = words;
+    words += region_words(b->W, I.cap, I.tsize);
+    words = (words + 31) & ~31ull;  // 256-byte aligned regions
+    I.epoch = 0;
+  }
+  uint64_t* np = nullptr;
+  BCUDA(cudaMalloc(&np, sizeof(uint64_t) * std::max<unsigned long long>(words, 1)));
+  BCUDA(cudaMemsetAsync(np, 0, sizeof(uint64_t) * std::max<unsigned long long>(words, 1), b->stream));
+  if (keep && b->pool) {
+    BInst* d_old = nullptr;
+    BCUDA(cudaMalloc(&d_old, sizeof(BInst) * b->ninst));
+    BCUDA(cudaMemcpyAsync(d_old, old.data(), sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+    BCUDA(cudaMemcpyAsync(b->d_inst, b->h_inst, sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+    BDISPATCH(b->W, launch_relocate, b, d_old, b->pool, np);
+    BCUDA(cudaGetLastError());
+    BCUDA(cudaStreamSynchronize(b->stream));
+    cudaFree(d_old);
+  }
+  BCUDA(cudaStreamSynchronize(b->stream));
+  cudaFree(b->pool);
+  b->pool = np;
+  b->pool_words = words;
+  b->layout_dirty = false;
+  drop_graphs(b);
+  return PPVM_OK;
+}
+
+// Resets every instance to its initial terms (uploaded packed, scattered by a kernel).
+ppvm_status load_initial(ppvm_batch* b) {
+  std::vector<unsigned long long> off(b->ninst);
+  std::vector<uint64_t> packed;
+  const int W = b->W;
+  for (size_t i = 0; i < b->ninst; ++i) {
+    const int wi = words_of(b->nq[i]);
+    const size_t k = b->ic[i].size();
+    off[i] = packed.size();
+    const size_t at = packed.size();
+    packed.resize(at + (2 * W + 1) * k, 0);
+    for (size_t t = 0; t < k; ++t)
+      for (int w = 0; w < wi; ++w) {
+        packed[at + t * W + w] = b->ix[i][t * wi + w];
+        packed[at + k * W + t * W + w] = b->iz[i][t * wi + w];
+      }
+    if (k) std::memcpy(&packed[at + 2 * k * W], b->ic[i].data(), sizeof(double) * k);
+    BInst& I = b->h_inst[i];
+    I.n = k;
+    I.pc = I.op_begin;
+    I.tgu = 0;
+    I.need = 0;
+    I.err = 0;
+    I.thr = b->thr[i];
+    I.maxw = b->maxw[i];
+  }
+  uint64_t* d_src = nullptr;
+  unsigned long long* d_off = nullptr;
+  BCUDA(cudaMalloc(&d_src, sizeof(uint64_t) * std::max<size_t>(packed.size(), 1)));
+  BCUDA(cudaMalloc(&d_off, sizeof(unsigned long long) * b->ninst));
+  if (!packed.empty())
+    BCUDA(cudaMemcpyAsync(d_src, packed.data(), sizeof(uint64_t) * packed.size(), cudaMemcpyHostToDevice, b->stream));
+  BCUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(unsigned long long) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+  BCUDA(cudaMemcpyAsync(b->d_inst, b->h_inst, sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+  BDISPATCH(b->W, launch_load, b, d_off, d_src);
+  BCUDA(cudaGetLastError());
+  BCUDA(cudaStreamSynchronize(b->stream));
+  cudaFree(d_src);
+  cudaFree(d_off);
+  return PPVM_OK;
+}
+
+// One CUDA graph per layer (layer index max_layers runs whatever follows the last boundary).
+ppvm_status ensure_graphs(ppvm_batch* b) {
+  const int cfg[3] = {b->block, b->items, b->W};
+  if (b->graphs.size() == (size_t)b->max_layers + 1 && std::equal(cfg, cfg + 3, b->graph_cfg)) return PPVM_OK;
+  drop_graphs(b);
+  for (uint32_t L = 0; L <= b->max_layers; ++L) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    BCUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t le = launch_any(b, (int)L);
+    const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return bfail(PPVM_ECUDA, std::string("layer graph capture failed: ") +
+                                   cudaGetErrorString(le != cudaSuccess ? le : ce));
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return bfail(PPVM_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    b->graphs.push_back(ge);
+  }
+  std::copy(cfg, cfg + 3, b->graph_cfg);
+  return PPVM_OK;
+}
+
+// After a launch sequence: grows the regions of instances that ran out of capacity.
+// Returns the first layer to relaunch through *first (UINT32_MAX when nothing failed).
+ppvm_status grow_failed(ppvm_batch* b, uint32_t* first) {
+  *first = 0xFFFFFFFFu;
+  bool grow = false;
+  for (size_t i = 0; i < b->ninst; ++i) {
+    BInst& I = b->h_inst[i];
+    if (!I.err) continue;
+    if (I.err != kErrCapacity)
+      return bfail(PPVM_ECUDA, "batch instance " + std::to_string(i) + ": device error " + std::to_string(I.err));
+    b->cap[i] = std::max<unsigned long long>(2 * b->cap[i], I.need + I.need / 2 + 64);
+    if (b->cap[i] >= 0xFFFFFFF0ull) return bfail(PPVM_ECAPACITY, "batch instance capacity limit (2^32) exceeded");
+    I.err = 0;
+    grow = true;
+    uint32_t L = 0;  // the layer holding the failing op
+    while (L < I.n_layers && b->lends[i][L] <= I.pc - I.op_begin) ++L;
+    *first = std::min(*first, L);
+  }
+  if (grow) BTRY(layout(b, true));
+  return PPVM_OK;
+}
+
+ppvm_status run_all(ppvm_batch* b, bool use_graphs, bool persistent) {
+  BCUDA(cudaSetDevice(b->device));
+  BTRY(upload_ops(b));
+  if (b->layout_dirty || !b->pool) BTRY(layout(b, false));
+  BTRY(load_initial(b));
+  uint32_t first = 0;
+  for (int attempt = 0; attempt < 64; ++attempt) {
+    if (persistent) {
+      BCUDA(launch_any(b, -1));
+    } else {
+      if (use_graphs) BTRY(ensure_graphs(b));
+      for (uint32_t L = first; L <= b->max_layers; ++L) {
+        if (use_graphs) BCUDA(cudaGraphLaunch(b->graphs[L], b->stream));
+        else BCUDA(launch_any(b, (int)L));
+      }
+    }
+    BCUDA(cudaMemcpyAsync(b->h_inst, b->d_inst, sizeof(BInst) * b->ninst, cudaMemcpyDeviceToHost, b->stream));
+    BCUDA(cudaStreamSynchronize(b->stream));
+    BTRY(grow_failed(b, &first));
+    if (first == 0xFFFFFFFFu) {
+      b->ran = true;
+      return PPVM_OK;
+    }
+  }
+  return bfail(PPVM_ECAPACITY, "batch capacity growth did not converge");
+}
+
+}  // namespace
+
+extern "C" {
+
+ppvm_status ppvm_batch_destroy(ppvm_batch* b) {
+  if (!b) return PPVM_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  drop_graphs(b);
+  cudaFree(b->d_inst);
+  cudaFreeHost(b->h_inst);
+  cudaFree(b->d_ops);
+  cudaFree(b->d_lends);
+  cudaFree(b->pool);
+  cudaFree(b->d_out);
+  if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_create(ppvm_batch** out, size_t n_inst, const uint32_t* n_qubits, const double* min_abs_coeff,
+                              const uint64_t* max_weight, uint32_t flags, int device) {
+  if (!out) return bfail(PPVM_EINVAL, "null out pointer");
+  *out = nullptr;
+  if (n_inst == 0 || n_inst > 65535 || !n_qubits || !min_abs_coeff || !max_weight)
+    return bfail(PPVM_EINVAL, "need 1..65535 instances and their n_qubits, min_abs_coeff, max_weight");
+  uint32_t nmax = 0;
+  for (size_t i = 0; i < n_inst; ++i) {
+    if (n_qubits[i] == 0 || n_qubits[i] > 512) return bfail(PPVM_EINVAL, "n_qubits must be in [1, 512]");
+    nmax = std::max(nmax, n_qubits[i]);
+  }
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return bfail(PPVM_ENODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= count) return bfail(PPVM_EINVAL, "device ordinal out of range");
+  BCUDA(cudaSetDevice(device));
+  ppvm_batch* b = new ppvm_batch();
+  b->device = device;
+  b->flags = flags;
+  b->ninst = n_inst;
+  b->W = batch_words(nmax);
+  b->nq.assign(n_qubits, n_qubits + n_inst);
+  b->thr.assign(min_abs_coeff, min_abs_coeff + n_inst);
+  b->maxw.assign(max_weight, max_weight + n_inst);
+  b->ix.resize(n_inst);
+  b->iz.resize(n_inst);
+  b->ic.resize(n_inst);
+  b->ops.resize(n_inst);
+  b->lends.resize(n_inst);
+  b->cap.assign(n_inst, 256);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&b->d_inst, sizeof(BInst) * n_inst) != cudaSuccess ||
+      cudaMallocHost(&b->h_inst, sizeof(BInst) * n_inst) != cudaSuccess ||
+      cudaMalloc(&b->d_out, sizeof(double) * n_inst) != cudaSuccess) {
+    ppvm_batch_destroy(b);
+    return bfail(PPVM_ECAPACITY, "device allocation failed");
+  }
+  std::memset(b->h_inst, 0, sizeof(BInst) * n_inst);
+  *out = b;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_set_stream(ppvm_batch* b, void* cuda_stream) {
+  if (!b) return bfail(PPVM_EINVAL, "null batch");
+  BCUDA(cudaSetDevice(b->device));
+  BCUDA(cudaStreamSynchronize(b->stream));
+  if (b->own_stream) cudaStreamDestroy(b->stream);
+  if (cuda_stream) {
+    b->stream = (cudaStream_t)cuda_stream;
+    b->own_stream = false;
+  } else {
+    BCUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    b->own_stream = true;
+  }
+  drop_graphs(b);
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_add_terms(ppvm_batch* b, size_t inst, const uint64_t* x, const uint64_t* z, const double* c,
+                                 size_t k) {
+  if (!b || inst >= b->ninst) return bfail(PPVM_EINVAL, "bad batch or instance index");
+  if (k && (!x || !z || !c)) return bfail(PPVM_EINVAL, "null term arrays");
+  const int wi = words_of(b->nq[inst]);
+  const int tail = (int)(b->nq[inst] % 64);
+  auto& X = b->ix[inst];
+  auto& Z = b->iz[inst];
+  auto& Cc = b->ic[inst];
+  for (size_t t = 0; t < k; ++t) {
+    if (tail && ((x[t * wi + wi - 1] | z[t * wi + wi - 1]) >> tail))
+      return bfail(PPVM_EINVAL, "word has bits set at or above n_qubits");
+    // `+=` into an insertion-ordered map (crates/ppvm-pauli-sum/src/sum/ops.rs:140-151)
+    size_t j = 0;
+    const size_t have = Cc.size();
+    for (; j < have; ++j) {
+      bool eq = true;
+      for (int w = 0; w < wi && eq; ++w) eq = X[j * wi + w] == x[t * wi + w] && Z[j * wi + w] == z[t * wi + w];
+      if (eq) break;
+    }
+    if (j < have) {
+      Cc[j] += c[t];
+    } else {
+      X.insert(X.end(), x + t * wi, x + (t + 1) * wi);
+      Z.insert(Z.end(), z + t * wi, z + (t + 1) * wi);
+      Cc.push_back(c[t]);
+    }
+  }
+  b->cap[inst] = std::max<unsigned long long>(b->cap[inst], 2 * Cc.size() + 64);
+  b->layout_dirty = true;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_set_ops(ppvm_batch* b, size_t inst, const ppvm_op* ops, size_t n_ops) {
+  if (!b || inst >= b->ninst) return bfail(PPVM_EINVAL, "bad batch or instance index");
+  if (n_ops && !ops) return bfail(PPVM_EINVAL, "null op list");
+  const uint32_t n = b->nq[inst];
+  const double half_pi = 1.5707963267948966;
+  std::vector<BOp> out;
+  std::vector<uint32_t> le;
+  int truncs = 0;
+  for (size_t i = 0; i < n_ops; ++i) {
+    const ppvm_op& op = ops[i];
+    if (op.flags != 0 || op.code >= PPVM_OP_COUNT_) return bfail(PPVM_EINVAL, "bad op code or flags");
+    BOp bo;
+    std::memset(&bo, 0, sizeof(bo));
+    if (op.code == PPVM_OP_TRUNCATE) {
+      bo.kind = B_TRUNC;
+      out.push_back(bo);
+      if (++truncs % 2 == 0) le.push_back((uint32_t)out.size());
+      continue;
+    }
+    const bool two = op.code == PPVM_OP_CNOT || op.code == PPVM_OP_CZ || op.code == PPVM_OP_CY ||
+                     op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY || op.code == PPVM_OP_RZZ ||
+                     op.code == PPVM_OP_DEPOLARIZE2;
+    if (op.q0 >= n || (two && (op.q1 >= n || op.q1 == op.q0)))
+      return bfail(PPVM_EINVAL, "qubit index out of range (or a two-qubit op on one qubit)");
+    DevOp& d = bo.d;
+    d.w0 = (uint16_t)(op.q0 >> 6);
+    d.b0 = (uint16_t)(op.q0 & 63);
+    d.w1 = (uint16_t)((two ? op.q1 : op.q0) >> 6);
+    d.b1 = (uint16_t)((two ? op.q1 : op.q0) & 63);
+    d.two = two ? 1 : 0;
+    const bool rot = op.code >= PPVM_OP_RX && op.code <= PPVM_OP_RZZ;
+    if (rot) {
+      const bool gx = op.code == PPVM_OP_RX || op.code == PPVM_OP_RY || op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY;
+      const bool gz = op.code == PPVM_OP_RZ || op.code == PPVM_OP_RY || op.code == PPVM_OP_RZZ || op.code == PPVM_OP_RYY;
+      d.ax = (uint16_t)((gx ? 1 : 0) | ((gx && two) ? 2 : 0));
+      d.az = (uint16_t)((gz ? 1 : 0) | ((gz && two) ? 2 : 0));
+      if ((b->flags & PPVM_FLAG_CLIFFORD_ANGLES) && (op.theta == half_pi || op.theta == -half_pi)) {
+        bo.kind = B_LOCAL;
+        d.code = C_ROTC;
+        d.f0 = op.theta > 0 ? 1.0 : -1.0;
+      } else {
+        bo.kind = B_ROT;
+        bo.sn = std::sin(op.theta);
+        bo.cs = std::cos(op.theta);
+      }
+    } else {
+      bo.kind = B_LOCAL;
+      switch (op.code) {
+        case PPVM_OP_X: d.code = C_X; break;
+        case PPVM_OP_Y: d.code = C_Y; break;
+        case PPVM_OP_Z: d.code = C_Z; break;
+        case PPVM_OP_H: d.code = C_H; break;
+        case PPVM_OP_S: d.code = C_S; break;
+        case PPVM_OP_S_DAG: d.code = C_SDAG; break;
+        case PPVM_OP_SQRT_X: d.code = C_SQX; break;
+        case PPVM_OP_SQRT_X_DAG: d.code = C_SQXDAG; break;
+        case PPVM_OP_SQRT_Y: d.code = C_SQY; break;
+        case PPVM_OP_SQRT_Y_DAG: d.code = C_SQYDAG; break;
+        case PPVM_OP_CNOT: d.code = C_CNOT; break;
+        case PPVM_OP_CZ: d.code = C_CZ; break;
+        case PPVM_OP_CY: d.code = C_CY; break;
+        case PPVM_OP_PAULI_ERROR: {  // noise.rs:17-37, factors as the per-op pass computes them
+          d.code = C_PAULI_ERROR;
+          const double one = 1.0;
+          d.f0 = one - op.p[1] * 2.0 - op.p[2] * 2.0;
+          d.f1 = one - op.p[0] * 2.0 - op.p[1] * 2.0;
+          d.f2 = one - op.p[0] * 2.0 - op.p[2] * 2.0;
+          break;
+        }
+        case PPVM_OP_DEPOLARIZE1: d.code = C_DEP1; d.f0 = 1.0 - op.theta * (4.0 / 3.0); break;
+        case PPVM_OP_DEPOLARIZE2: d.code = C_DEP2; d.f0 = 1.0 - op.theta * (16.0 / 15.0); break;
+        default: return bfail(PPVM_EINVAL, "unsupported op in a batch");
+      }
+    }
+    out.push_back(bo);
+  }
+  b->ops[inst] = std::move(out);
+  b->lends[inst] = std::move(le);
+  b->ops_dirty = true;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_set_config(ppvm_batch* b, int block, int items, int table_factor) {
+  if (!b) return bfail(PPVM_EINVAL, "null batch");
+  if ((block != 128 && block != 256 && block != 512) || (items != 2 && items != 4) ||
+      (table_factor != 2 && table_factor != 4))
+    return bfail(PPVM_EINVAL, "block in {128, 256, 512}, items in {2, 4}, table_factor in {2, 4}");
+  if (table_factor != b->tfac) b->layout_dirty = true;
+  b->block = block;
+  b->items = items;
+  b->tfac = table_factor;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_get_config(const ppvm_batch* b, int* block, int* items, int* table_factor) {
+  if (!b || !block || !items || !table_factor) return bfail(PPVM_EINVAL, "null argument");
+  *block = b->block;
+  *items = b->items;
+  *table_factor = b->tfac;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_run(ppvm_batch* b) {
+  if (!b) return bfail(PPVM_EINVAL, "null batch");
+  return run_all(b, true, false);
+}
+
+ppvm_status ppvm_batch_run_persistent(ppvm_batch* b) {
+  if (!b) return bfail(PPVM_EINVAL, "null batch");
+  return run_all(b, false, true);
+}
+
+ppvm_status ppvm_batch_autotune(ppvm_batch* b, int* block, int* items, int* table_factor, double* best_ms) {
+  if (!b) return bfail(PPVM_EINVAL, "null batch");
+  BCUDA(cudaSetDevice(b->device));
+  BTRY(run_all(b, true, false));  // sizes every region to its peak first
+  const int blocks[3] = {128, 256, 512}, its[2] = {2, 4}, tfs[2] = {2, 4};
+  double best = 1e300;
+  int bb = b->block, bi = b->items, bt = b->tfac;
+  cudaEvent_t e0, e1;
+  BCUDA(cudaEventCreate(&e0));
+  BCUDA(cudaEventCreate(&e1));
+  for (int tf : tfs)
+    for (int bl : blocks)
+      for (int it : its) {
+        BTRY(ppvm_batch_set_config(b, bl, it, tf));
+        BTRY(run_all(b, true, false));  // warm: graphs captured, layout fixed
+        BCUDA(cudaEventRecord(e0, b->stream));
+        BTRY(run_all(b, true, false));
+        BCUDA(cudaEventRecord(e1, b->stream));
+        BCUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        BCUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+          best = ms;
+          bb = bl;
+          bi = it;
+          bt = tf;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  BTRY(ppvm_batch_set_config(b, bb, bi, bt));
+  BTRY(run_all(b, true, false));
+  if (block) *block = bb;
+  if (items) *items = bi;
+  if (table_factor) *table_factor = bt;
+  if (best_ms) *best_ms = best;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_overlap_with_zero(ppvm_batch* b, double* out) {
+  if (!b || !out) return bfail(PPVM_EINVAL, "null argument");
+  if (!b->ran) return bfail(PPVM_EINVAL, "run the batch first");
+  BCUDA(cudaSetDevice(b->device));
+  BDISPATCH(b->W, launch_owz, b);
+  BCUDA(cudaGetLastError());
+  BCUDA(cudaMemcpyAsync(out, b->d_out, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost, b->stream));
+  BCUDA(cudaStreamSynchronize(b->stream));
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_len(const ppvm_batch* b, size_t inst, size_t* out) {
+  if (!b || !out || inst >= b->ninst) return bfail(PPVM_EINVAL, "bad argument");
+  *out = b->ran ? (size_t)b->h_inst[inst].n : b->ic[inst].size();
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_term_gate_updates(const ppvm_batch* b, uint64_t* per_inst, uint64_t* total) {
+  if (!b) return bfail(PPVM_EINVAL, "null batch");
+  uint64_t t = 0;
+  for (size_t i = 0; i < b->ninst; ++i) {
+    const uint64_t v = b->ran ? b->h_inst[i].tgu : 0;
+    if (per_inst) per_inst[i] = v;
+    t += v;
+  }
+  if (total) *total = t;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_export_terms(ppvm_batch* b, size_t inst, uint64_t* x, uint64_t* z, double* c, size_t cap,
+                                    size_t* n_out) {
+  if (!b || !n_out || inst >= b->ninst) return bfail(PPVM_EINVAL, "bad argument");
+  if (!b->ran) return bfail(PPVM_EINVAL, "run the batch first");
+  const BInst& I = b->h_inst[inst];
+  const size_t n = std::min<size_t>(cap, I.n);
+  *n_out = n;
+  if (n == 0) return PPVM_OK;
+  if (!x || !z || !c) return bfail(PPVM_EINVAL, "null output arrays");
+  BCUDA(cudaSetDevice(b->device));
+  const int W = b->W, wi = words_of(b->nq[inst]);
+  std::vector<uint64_t> buf((size_t)(2 * W) * n);
+  const uint64_t* base = b->pool + I.off;
+  for (int w = 0; w < 2 * W; ++w)
+    BCUDA(cudaMemcpyAsync(buf.data() + (size_t)w * n, base + (size_t)w * I.cap, sizeof(uint64_t) * n,
+                          cudaMemcpyDeviceToHost, b->stream));
+  BCUDA(cudaMemcpyAsync(c, base + (size_t)2 * W * I.cap, sizeof(double) * n, cudaMemcpyDeviceToHost, b->stream));
+  BCUDA(cudaStreamSynchronize(b->stream));
+  for (size_t i = 0; i < n; ++i)
+    for (int w = 0; w < wi; ++w) {
+      x[i * wi + w] = buf[(size_t)w * n + i];
+      z[i * wi + w] = buf[(size_t)(W + w) * n + i];
+    }
+  return PPVM_OK;
+}
+
+}  // extern "C"

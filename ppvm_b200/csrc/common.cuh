@@ -85,7 +85,7 @@ __device__ __forceinline__ unsigned long long pack_state(unsigned epoch, unsigne
 // Exclusive prefix of tile `tile` given its aggregate.  All threads of the block call it;
 // warp 0 publishes and looks back.  Every wait is bounded; on timeout the error flag is set
 // and a (wrong) prefix is returned so that the kernel ends.
-__device__ unsigned long long lookback(unsigned long long* ts, unsigned tile,
+static __device__ unsigned long long lookback(unsigned long long* ts, unsigned tile,
                                        unsigned long long agg, unsigned epoch, Ctrl* ctrl,
                                        int op, unsigned long long* s_slot) {
   if (threadIdx.x < 32) {

@@ -273,7 +273,7 @@ k_rot_apply(Planes P, Ctrl* ctrl, Gen g, double sn, double cs, const uint32_t* s
 }
 
 // Publishes the live count after a rotation and resets the tile tickets (one thread).
-__global__ void k_commit_rot(Ctrl* ctrl, int op, OpLog* log) {
+static __global__ void k_commit_rot(Ctrl* ctrl, int op, OpLog* log) {
   for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
   if (ctrl->err) return;
   const unsigned long long nchild = ctrl->n_s - 2 * ctrl->n_pairs;
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(256) k_owz(Planes P, const Ctrl* ctrl, double*
   if (threadIdx.x == 0) partials[blockIdx.x] = b;
 }
 
-__global__ void k_sum_partials(const double* partials, int n, Ctrl* ctrl) {
+static __global__ void k_sum_partials(const double* partials, int n, Ctrl* ctrl) {
   __shared__ double s_red[8];
   double acc = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) acc = __dadd_rn(acc, partials[i]);

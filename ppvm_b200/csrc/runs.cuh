@@ -223,7 +223,7 @@ k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long lo
   }
 }
 
-__global__ void __launch_bounds__(256) k_run_scatter(Ctrl* ctrl, RunScratch R) {
+static __global__ void __launch_bounds__(256) k_run_scatter(Ctrl* ctrl, RunScratch R) {
   if (ld_volatile_int(&ctrl->err)) return;
   const unsigned long long N = ld_volatile(&ctrl->n);
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
@@ -474,7 +474,7 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
 }
 
 // Publishes the count after the run and fills the op log of its gates (and its TRUNCATE).
-__global__ void k_run_commit(Ctrl* ctrl, RunScratch R, int op0, int L, int trunc_op, OpLog* log) {
+static __global__ void k_run_commit(Ctrl* ctrl, RunScratch R, int op0, int L, int trunc_op, OpLog* log) {
   for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
   if (ctrl->err) return;
   const unsigned long long n0 = ctrl->n;

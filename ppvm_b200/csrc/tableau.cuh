@@ -25,7 +25,7 @@ constexpr int kTabBlock = 256;
 constexpr size_t kTabMaxSmem = 160 * 1024;
 
 // ---- per-gate rules over "bit vectors" B: bool (one word) or uint64_t (64 words at once) ----
-__host__ __device__ __forceinline__ bool bnot(bool b) { return !b; }
+__host__ __device__ __forceinline__ bool bnot(int b) { return !b; }  // bool operands promote to int
 __host__ __device__ __forceinline__ uint64_t bnot(uint64_t b) { return ~b; }
 template <class B>
 __host__ __device__ __forceinline__ B bconst(bool v);
@@ -214,7 +214,7 @@ k_tableau(Planes P, Planes O, Ctrl* ctrl, TabParams tp, const uint64_t* __restri
 }
 
 // Publishes the count after a tableau pass (and fills the log of its fused TRUNCATE).
-__global__ void k_commit_tableau(Ctrl* ctrl, int trunc_op, OpLog* log) {
+static __global__ void k_commit_tableau(Ctrl* ctrl, int trunc_op, OpLog* log) {
   for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
   if (ctrl->err) return;
   const unsigned long long n_in = ctrl->n, n_out = ctrl->n_s;
