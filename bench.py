@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ppvm_b200", choices=["ppvm_b200", "reference"])
     ap.add_argument("--layers", type=int, default=20)
+    ap.add_argument("--workload", default="kicked_ising_2d", choices=["kicked_ising_2d", "batched_tfim"],
+                    help="kicked_ising_2d: one 12x12 sum (headline); batched_tfim: 256 independent 1D TFIM "
+                         "instances through the batched engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-launch-events", action="store_true",
                     help="time the steps without per-launch CUDA events (no kernel breakdown)")
@@ -305,9 +308,158 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+BATCH_CPU_SAMPLE = 64  # instances of the batched workload timed on the host CPU
+
+
+def batched_config(n_inst, world, extra=None):
+    d = {"workload": f"batched_tfim: {n_inst} independent 1D TFIM instances (seed 1), n ~ U[16,128], "
+                     "steps ~ U[5,30], h ~ U[0.5,1.5], J=1, dt=0.05, obs Z(n/2), thr 1e-5",
+         "instances": n_inst, "parallelism": f"replicas x{world}" if world > 1 else "one batch"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def batched_cpu(wls):
+    from oracle.pyoracle import OracleSum
+
+    t0 = time.perf_counter()
+    tgu = 0
+    for w in wls:
+        o = OracleSum(w.n_qubits, w.min_abs_coeff, w.max_weight)
+        x, z = G.parse_word(w.observable[0][0], w.n_qubits)
+        o.add_terms(x[None], z[None], np.array([w.observable[0][1]]))
+        tgu += C.term_gate_updates(o.run_ops(w.ops, counts=True), w.ops)
+        o.overlap_with_zero()
+    return tgu, time.perf_counter() - t0
+
+
+def run_batched_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    wls = C.batched_tfim()[:BATCH_CPU_SAMPLE]
+    for _ in range(args.warmup):
+        batched_cpu(wls[:8])
+    tot_u, tot_t = 0, 0.0
+    for _ in range(args.steps):
+        u, dt = batched_cpu(wls)
+        tot_u += u
+        tot_t += dt
+    v = tot_u / tot_t
+    line = {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated circuits)",
+            "config": batched_config(BATCH_CPU_SAMPLE, 1, {"note": "first 64 instances per step on the host CPU"}),
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": "port",
+                             "sample": f"first {BATCH_CPU_SAMPLE} of the 256 instances per step"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_batched(args):
+    import torch
+    import torch.distributed as dist
+
+    from ppvm_b200.batch import PauliSumBatch
+    from ppvm_b200.paulisum import PauliSum
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    wls = C.batched_tfim()
+    b = PauliSumBatch.from_workloads(wls, device=local)
+    b.set_stream(stream.cuda_stream)
+    tune = b.autotune()  # warm-up: sizes every region, captures the layer graphs, picks the launch config
+    for _ in range(max(args.warmup, 1)):
+        b.run()
+    per, tgu = b.term_gate_updates()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            ev[i][0].record(stream)
+            b.run()
+            owz = b.overlap_with_zero()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    dev_s = sum(a.elapsed_time(c) for a, c in ev) / 1e3
+    # end to end: the batch built from the host circuits, run, <O> of every instance read back
+    e2e_s = 0.0
+    h2d = d2h = 0
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        b2 = PauliSumBatch.from_workloads(wls, device=local)
+        b2.set_config(tune["block"], tune["items"], tune["table_factor"])
+        b2.run()
+        b2.overlap_with_zero()
+        e2e_s += time.perf_counter() - t
+        h2d, d2h = b2.transfer_counters()
+        del b2
+    # the same instances one after another through the plain single-sum engine
+    seq = None
+    if rank == 0 and not args.no_cpu_baseline:
+        t = time.perf_counter()
+        for w in wls:
+            s = PauliSum([w.observable[0][0]], w.n_qubits, [1.0], min_abs_coeff=w.min_abs_coeff, device=local)
+            s.run(w.ops)
+            s.overlap_with_zero()
+        seq_s = time.perf_counter() - t
+        seq = {"value": tgu / seq_s, "unit": METRIC, "ms_to_all_O": 1e3 * seq_s,
+               "what": "the 256 instances one after another through the plain single-sum engine (PauliSum)"}
+    t_dev = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
+    dev_s, e2e_s = float(t_dev[0]), float(t_dev[1])
+    if rank == 0:
+        peak_gbs, peak_kind = measured_peak()
+        # algorithmic bytes: every term-gate update reads the X and Z word holding the gate's qubit
+        achieved = 16.0 * tgu * args.steps / dev_s / 1e9
+        line = {"metric": METRIC, "value": tgu * args.steps * world / dev_s, "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (generated circuits)",
+                "config": batched_config(len(wls), world, {"l2": "flushed between steps (256 MB write)",
+                                                           "term_gate_updates_per_step": tgu,
+                                                           "launch_config": tune,
+                                                           "max_live_terms": int(max(b.len_of(j) for j in range(len(wls))))}),
+                "e2e": {"value": tgu * args.steps * world / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_s / args.steps},
+                "time_to_all_O_ms": 1e3 * dev_s / args.steps,
+                "sequential_plain_gpu": seq,
+                "gpu_launches": (max(w.meta["steps"] for w in wls) + 1 + 1) * args.steps,
+                "roofline": {"bound": "latency", "kernel": "k_batch", "achieved": achieved, "peak": peak_gbs,
+                             "unit": "GB/s", "frac": achieved / peak_gbs, "peak_kind": peak_kind, "traffic": None,
+                             "note": "16 B per term-gate update; one CTA per instance, the largest instance sets the time"},
+                "clocks": clk.summary()}
+        if world == 1 and not args.no_cpu_baseline:
+            u, dt = batched_cpu(wls[:BATCH_CPU_SAMPLE])
+            line["cpu_baseline"] = {"value": u / dt, "unit": METRIC, "cores": 1, "kind": "port",
+                                    "sample": f"first {BATCH_CPU_SAMPLE} of the 256 instances, single-thread C++ "
+                                              f"restatement of the reference PauliSum ({dt:.1f} s)"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "batched_tfim":
+        run_batched_reference(args) if args.impl == "reference" else run_batched(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -255,6 +255,8 @@ ppvm_status ppvm_batch_len(const ppvm_batch* batch, size_t inst, size_t* out);
 ppvm_status ppvm_batch_export_terms(ppvm_batch* batch, size_t inst, uint64_t* x, uint64_t* z,
                                     double* c, size_t cap, size_t* n_out);
 ppvm_status ppvm_batch_term_gate_updates(const ppvm_batch* batch, uint64_t* per_inst, uint64_t* total);
+/* Bytes this batch has copied host->device and device->host since it was created. */
+ppvm_status ppvm_batch_transfer_counters(const ppvm_batch* batch, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
 /* ---- diagnostics ------------------------------------------------------------------- */
 /* Thread-local text of the last failing call ("" if none). */

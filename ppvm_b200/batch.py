@@ -127,6 +127,12 @@ class PauliSumBatch:
         n = self.instances[j].n_qubits
         return [(G.word_str(x[i], z[i], n), float(c[i])) for i in range(len(c))]
 
+    def transfer_counters(self) -> tuple[int, int]:
+        """Bytes copied host->device and device->host by this batch since it was created."""
+        h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(lib().ppvm_batch_transfer_counters(self._h, ctypes.byref(h2d), ctypes.byref(d2h)))
+        return int(h2d.value), int(d2h.value)
+
     def term_gate_updates(self):
         per = np.zeros(len(self), dtype=np.uint64)
         tot = ctypes.c_uint64()

@@ -103,6 +103,18 @@ def kicked_ising_2d(L: int = 12, layers: int = 20, theta_h=0.6, theta_zz: float 
                     meta={"L": L, "layers": layers, "bonds": len(bonds)})
 
 
+def kicked_ising_random_h(L: int = 10, layers: int = 30, seed: int = 2, lo: float = 0.4, hi: float = 0.8,
+                          thr: float = 1e-7, max_weight: int | None = None, obs=(5, 5)) -> Workload:
+    """2D kicked Ising with a seeded transverse angle per layer, theta_h ~ U[lo, hi]
+    (splitmix64), RZZ(-pi/2) on every bond; observable Z at ``obs``."""
+    rng = SplitMix64(seed)
+    th = [rng.uniform_range(lo, hi) for _ in range(layers)]
+    wl = kicked_ising_2d(L=L, layers=layers, theta_h=th, thr=thr, max_weight=max_weight, obs=obs)
+    wl.name = f"kicked_ising_{L}x{L}_layers{layers}_seed{seed}"
+    wl.meta["theta_h"] = th
+    return wl
+
+
 def clifford_t(n: int = 64, layers: int = 1000, seed: int = 0, p_t: float = 0.05, thr: float = 1e-6) -> Workload:
     """Random Clifford+T brickwork.  Forward layer: each qubit one of {H, S, S_DAG}; CNOT on
     (2i, 2i+1) for even layers, (2i+1, 2i+2) for odd ones; then T = RZ(pi/4) on each qubit with

@@ -584,6 +584,7 @@ struct ppvm_batch {
   int graph_cfg[3] = {0, 0, 0};
   uint32_t max_layers = 0;
   bool ran = false;
+  unsigned long long xfer_h2d = 0, xfer_d2h = 0;  // bytes copied host<->device since creation
 };
 
 namespace {
@@ -675,6 +676,7 @@ ppvm_status upload_ops(ppvm_batch* b) {
   BCUDA(cudaMalloc(&b->d_lends, sizeof(uint32_t) * std::max<size_t>(le.size(), 1)));
   if (!all.empty())
     BCUDA(cudaMemcpyAsync(b->d_ops, all.data(), sizeof(BOp) * all.size(), cudaMemcpyHostToDevice, b->stream));
+  b->xfer_h2d += sizeof(BOp) * all.size() + sizeof(uint32_t) * le.size();
   if (!le.empty())
     BCUDA(cudaMemcpyAsync(b->d_lends, le.data(), sizeof(uint32_t) * le.size(), cudaMemcpyHostToDevice, b->stream));
   BCUDA(cudaStreamSynchronize(b->stream));
@@ -704,6 +706,7 @@ ppvm_status layout(ppvm_batch* b, bool keep) {
     BCUDA(cudaMalloc(&d_old, sizeof(BInst) * b->ninst));
     BCUDA(cudaMemcpyAsync(d_old, old.data(), sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
     BCUDA(cudaMemcpyAsync(b->d_inst, b->h_inst, sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+    b->xfer_h2d += 2 * sizeof(BInst) * b->ninst;
     BDISPATCH(b->W, launch_relocate, b, d_old, b->pool, np);
     BCUDA(cudaGetLastError());
     BCUDA(cudaStreamSynchronize(b->stream));
@@ -752,6 +755,7 @@ ppvm_status load_initial(ppvm_batch* b) {
     BCUDA(cudaMemcpyAsync(d_src, packed.data(), sizeof(uint64_t) * packed.size(), cudaMemcpyHostToDevice, b->stream));
   BCUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(unsigned long long) * b->ninst, cudaMemcpyHostToDevice, b->stream));
   BCUDA(cudaMemcpyAsync(b->d_inst, b->h_inst, sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+  b->xfer_h2d += sizeof(uint64_t) * packed.size() + sizeof(unsigned long long) * b->ninst + sizeof(BInst) * b->ninst;
   BDISPATCH(b->W, launch_load, b, d_off, d_src);
   BCUDA(cudaGetLastError());
   BCUDA(cudaStreamSynchronize(b->stream));
@@ -825,6 +829,7 @@ ppvm_status run_all(ppvm_batch* b, bool use_graphs, bool persistent) {
     }
     BCUDA(cudaMemcpyAsync(b->h_inst, b->d_inst, sizeof(BInst) * b->ninst, cudaMemcpyDeviceToHost, b->stream));
     BCUDA(cudaStreamSynchronize(b->stream));
+    b->xfer_d2h += sizeof(BInst) * b->ninst;
     BTRY(grow_failed(b, &first));
     if (first == 0xFFFFFFFFu) {
       b->ran = true;
@@ -1104,6 +1109,14 @@ ppvm_status ppvm_batch_overlap_with_zero(ppvm_batch* b, double* out) {
   BCUDA(cudaGetLastError());
   BCUDA(cudaMemcpyAsync(out, b->d_out, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost, b->stream));
   BCUDA(cudaStreamSynchronize(b->stream));
+  b->xfer_d2h += sizeof(double) * b->ninst;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_transfer_counters(const ppvm_batch* b, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+  if (!b || !h2d_bytes || !d2h_bytes) return bfail(PPVM_EINVAL, "null argument");
+  *h2d_bytes = b->xfer_h2d;
+  *d2h_bytes = b->xfer_d2h;
   return PPVM_OK;
 }
 
