@@ -215,6 +215,37 @@ ppvm_status ppvm_transfer_counters(const ppvm_sum* sum, uint64_t* h2d_bytes, uin
 /* Kernels this handle has launched since it was created (all families, readouts included). */
 ppvm_status ppvm_launch_count(const ppvm_sum* sum, uint64_t* out);
 
+/* ---- term-budget and learned truncation ---------------------------------------------- */
+/* No counterpart in the reference, which truncates by |coefficient| and Pauli weight only
+ * (`crates/ppvm-pauli-sum/src/strategy.rs:12-170`).  A term-budget truncation keeps the
+ * `budget` terms of highest priority (exactly budget when the sum is larger), in order.
+ * Priority is |c| (mlp = NULL) or the score of a term-priority network: a BF16 tensor-core
+ * MLP 8 -> 64 -> 64 -> 1 (GELU) over per-term features, trained to predict
+ * log10 |contribution of the term to <O>|.  Features, for a sum on an L x L lattice (qubit
+ * r*L + c) with `layers_left` layers still to apply: weight/16, (log10|c| + 6)/6,
+ * layers_left/8, #X/8, #Y/8, #Z/8, nearest-neighbour bonds inside the support/8,
+ * weight*layers_left/64.  digit_bits (8 or 11; 0 = 8) is the radix-select digit width. */
+typedef struct ppvm_mlp ppvm_mlp; /* opaque */
+ppvm_status ppvm_truncate_budget(ppvm_sum* sum, uint64_t budget, const ppvm_mlp* mlp,
+                                 uint32_t lattice_l, uint32_t layers_left, int digit_bits);
+/* Features of the current terms, in iteration order: out[i*8 + k], up to cap rows. */
+ppvm_status ppvm_term_features(ppvm_sum* sum, uint32_t lattice_l, uint32_t layers_left, float* out,
+                               size_t cap, size_t* n_out);
+/* The network: 4801 FP32 parameters (W1[64][8], b1[64], W2[64][64], b2[64], w3[64], b3),
+ * seeded uniform initialisation.  Training runs on the device: per minibatch one
+ * forward+backward kernel (squared error on the targets) and one Adam step (beta 0.9,
+ * 0.999); samples are shuffled every epoch with a seeded permutation.  ppvm_mlp_grad
+ * returns the gradient of the mean squared error over all n samples without updating. */
+ppvm_status ppvm_mlp_create(ppvm_mlp** out, uint64_t seed, int device);
+ppvm_status ppvm_mlp_destroy(ppvm_mlp* mlp);
+ppvm_status ppvm_mlp_set_params(ppvm_mlp* mlp, const float* params, size_t n);
+ppvm_status ppvm_mlp_get_params(const ppvm_mlp* mlp, float* params, size_t n);
+ppvm_status ppvm_mlp_train(ppvm_mlp* mlp, const float* feats, const float* targets, size_t n, int epochs,
+                           int batch, float lr, uint64_t seed, float* last_epoch_loss);
+ppvm_status ppvm_mlp_grad(ppvm_mlp* mlp, const float* feats, const float* targets, size_t n, float* grads,
+                          float* loss);
+ppvm_status ppvm_mlp_predict(ppvm_mlp* mlp, const float* feats, size_t n, float* out);
+
 /* ---- batches of independent sums ----------------------------------------------------- */
 /* Many independent PauliSums (instances), each with its own qubit count, truncation
  * strategy, initial terms and gate list, advanced together on one GPU: one CTA per

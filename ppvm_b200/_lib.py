@@ -78,6 +78,17 @@ _SIGS = {
                               ctypes.POINTER(ctypes.c_uint8)],
     "ppvm_transfer_counters": [_P, _U64P, _U64P],
     "ppvm_launch_count": [_P, _U64P],
+    "ppvm_truncate_budget": [_P, ctypes.c_uint64, _P, ctypes.c_uint32, ctypes.c_uint32, _I],
+    "ppvm_term_features": [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), _SZ, _SZP],
+    "ppvm_mlp_create": [ctypes.POINTER(_P), ctypes.c_uint64, _I],
+    "ppvm_mlp_destroy": [_P],
+    "ppvm_mlp_set_params": [_P, ctypes.POINTER(ctypes.c_float), _SZ],
+    "ppvm_mlp_get_params": [_P, ctypes.POINTER(ctypes.c_float), _SZ],
+    "ppvm_mlp_train": [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), _SZ, _I, _I,
+                       ctypes.c_float, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)],
+    "ppvm_mlp_grad": [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), _SZ,
+                      ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
+    "ppvm_mlp_predict": [_P, ctypes.POINTER(ctypes.c_float), _SZ, ctypes.POINTER(ctypes.c_float)],
     "ppvm_batch_create": [ctypes.POINTER(_P), _SZ, _U32P, _DP, _U64P, ctypes.c_uint32, _I],
     "ppvm_batch_destroy": [_P],
     "ppvm_batch_set_stream": [_P, _P],

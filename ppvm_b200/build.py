@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libppvm_cuda.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "batch.cu", "noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "batch.cu", "learned.cu", "noalloc.cu")]
 HEADERS = sorted(
     os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc")) if f.endswith(".cuh")
 ) + [os.path.join(ROOT, "include", "ppvm_cuda.h")]

@@ -20,6 +20,7 @@
 #include "../../include/ppvm_cuda.h"
 #include "runs.cuh"
 #include "tableau.cuh"
+#include "budget.cuh"
 
 using namespace ppvm;
 
@@ -101,6 +102,9 @@ struct StageChunk {
 namespace ppvm {
 // Lets other translation units of the library set the text of ppvm_last_error_string().
 void set_last_error(const std::string& msg) { g_err = msg; }
+// The term-priority network's device weights and device (learned.cu).
+const MlpWeights* mlp_device_weights(const ppvm_mlp* m);
+int mlp_device(const ppvm_mlp* m);
 }  // namespace ppvm
 
 struct ppvm_sum {
@@ -139,6 +143,8 @@ struct ppvm_sum {
   PatItem* d_pat = nullptr;
   double* d_partials = nullptr;
   unsigned long long* d_counter = nullptr;
+  SelState* d_sel = nullptr;   // radix select state of budget truncation
+  unsigned* d_hist = nullptr;  // its digit histogram (2^11 bins, kept zero between uses)
   uint64_t* d_pres_keys = nullptr;
   int* d_pres_table = nullptr;
   unsigned pres_mask = 0;
@@ -672,7 +678,7 @@ struct K {
     }
     {
       ProfScope ps(s, F_RUN_COMMIT, op0, L);
-      k_run_commit<<<1, 1, 0, s->stream>>>(s->d_ctrl, s->R, op0, L, trunc_op, s->d_log);
+      k_run_commit<<<1, kRunMaxGates, 0, s->stream>>>(s->d_ctrl, s->R, op0, L, trunc_op, s->d_log);
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);
@@ -713,6 +719,35 @@ struct K {
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);
     return PPVM_OK;
+  }
+
+  // Term-budget truncation: priority keys, radix select of the budget-th largest, compaction.
+  static void budget(ppvm_sum* s, unsigned long long B, const MlpWeights* mw, int L, int layers_left, int bits) {
+    const Planes P = s->planes_view();
+    uint32_t* keys = s->s_idx;  // cap entries, free outside the rotation pipeline
+    const unsigned long long nub = std::max<unsigned long long>(s->n_host, 1);
+    k_score<W><<<grid_for(nub, 128, 8), 128, 0, s->stream>>>(P, s->d_ctrl, mw, L, layers_left, keys);
+    k_sel_init<<<1, 1, 0, s->stream>>>(s->d_ctrl, B, s->d_sel);
+    if (bits == 11) {
+      for (int shift : {21, 10, 0}) {
+        k_sel_hist<11><<<grid_for(nub, 256, 4), 256, 0, s->stream>>>(s->d_ctrl, keys, s->d_sel, shift, s->d_hist);
+        k_sel_pick<11><<<1, 256, 0, s->stream>>>(s->d_sel, shift, s->d_hist);
+      }
+    } else {
+      for (int shift : {24, 16, 8, 0}) {
+        k_sel_hist<8><<<grid_for(nub, 256, 4), 256, 0, s->stream>>>(s->d_ctrl, keys, s->d_sel, shift, s->d_hist);
+        k_sel_pick<8><<<1, 256, 0, s->stream>>>(s->d_sel, shift, s->d_hist);
+      }
+    }
+    const unsigned ea = s->next_tile_epoch(), eb = s->next_tile_epoch();
+    k_budget_compact<W, kScanBlock, ITEMS><<<grid_for(nub, TILE, 8), kScanBlock, 0, s->stream>>>(
+        P, s->d_ctrl, keys, s->d_sel, s->tstate, ea, s->tstate2, eb);
+    k_commit_budget<<<1, 1, 0, s->stream>>>(s->d_ctrl, s->d_sel);
+    s->launch_count += 3 + 2 * (bits == 11 ? 3 : 4) + 1;
+  }
+  static void features(ppvm_sum* s, int L, int layers_left, float* out) {
+    k_features<W><<<grid_for(std::max<unsigned long long>(s->n_host, 1), 256, 8), 256, 0, s->stream>>>(
+        s->planes_view(), s->d_ctrl, L, layers_left, out);
   }
 
   static void owz(ppvm_sum* s, int nblocks) {
@@ -1109,10 +1144,13 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
       cudaMallocHost(&s->h_ctrl, sizeof(Ctrl)) != cudaSuccess ||
       cudaMalloc(&s->d_partials, sizeof(double) * 8192) != cudaSuccess ||
       cudaMalloc(&s->d_counter, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&s->d_sel, sizeof(SelState)) != cudaSuccess ||
+      cudaMalloc(&s->d_hist, sizeof(unsigned) * 2048) != cudaSuccess ||
       cudaMalloc(&s->side, sizeof(uint64_t) * (2 * s->W + 1) * (kMaxPreserve + 1)) != cudaSuccess)
     return bail(fail(PPVM_ECAPACITY, "device allocation failed"));
   std::memset(s->h_ctrl, 0, sizeof(Ctrl));
-  if (cudaMemsetAsync(s->d_ctrl, 0, sizeof(Ctrl), s->stream) != cudaSuccess)
+  if (cudaMemsetAsync(s->d_hist, 0, sizeof(unsigned) * 2048, s->stream) != cudaSuccess ||
+      cudaMemsetAsync(s->d_ctrl, 0, sizeof(Ctrl), s->stream) != cudaSuccess)
     return bail(fail(PPVM_ECUDA, "memset failed"));
   ppvm_status st = grow(s, std::max<size_t>(capacity_hint, 4096));
   if (st != PPVM_OK) return bail(st);
@@ -1151,6 +1189,8 @@ ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
   cudaFree(s->d_pat);
   cudaFree(s->d_partials);
   cudaFree(s->d_counter);
+  cudaFree(s->d_sel);
+  cudaFree(s->d_hist);
   cudaFree(s->d_pres_keys);
   cudaFree(s->d_pres_table);
   if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
@@ -1628,6 +1668,53 @@ ppvm_status ppvm_transfer_counters(const ppvm_sum* s, uint64_t* h2d_bytes, uint6
 ppvm_status ppvm_launch_count(const ppvm_sum* s, uint64_t* out) {
   if (!s || !out) return fail(PPVM_EINVAL, "null argument");
   *out = s->launch_count;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_term_features(ppvm_sum* s, uint32_t lattice_l, uint32_t layers_left, float* out, size_t cap,
+                               size_t* n_out) {
+  if (!s || !n_out) return fail(PPVM_EINVAL, "null argument");
+  if (lattice_l > 0 && (uint64_t)lattice_l * lattice_l > s->n) return fail(PPVM_EINVAL, "lattice larger than the sum");
+  PPVM_TRY(ensure_device(s->device));
+  const size_t n = std::min<size_t>(cap, s->n_host);
+  *n_out = n;
+  if (n == 0) return PPVM_OK;
+  if (!out) return fail(PPVM_EINVAL, "null output");
+  float* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, sizeof(float) * kMlpIn * std::max<unsigned long long>(s->n_host, 1)));
+  DISPATCH_W(s->W, features(s, (int)lattice_l, (int)layers_left, d));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, sizeof(float) * kMlpIn * n, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(PPVM_ECUDA, std::string("term features: ") + cudaGetErrorString(e));
+  s->xfer_d2h += sizeof(float) * kMlpIn * n;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_truncate_budget(ppvm_sum* s, uint64_t budget, const ppvm_mlp* mlp, uint32_t lattice_l,
+                                 uint32_t layers_left, int digit_bits) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  if (digit_bits == 0) digit_bits = 8;
+  if (digit_bits != 8 && digit_bits != 11) return fail(PPVM_EINVAL, "digit_bits must be 8 or 11");
+  if (lattice_l > 0 && (uint64_t)lattice_l * lattice_l > s->n) return fail(PPVM_EINVAL, "lattice larger than the sum");
+  if (s->poisoned) return fail(PPVM_ECUDA, "sum is in an error state from an earlier failure");
+  PPVM_TRY(ensure_device(s->device));
+  const MlpWeights* mw = nullptr;
+  if (mlp) {
+    if (mlp_device(mlp) != s->device) return fail(PPVM_EINVAL, "network and sum live on different devices");
+    mw = mlp_device_weights(mlp);
+  }
+  if (s->n_host <= budget) return PPVM_OK;
+  DISPATCH_W(s->W, budget(s, budget, mw, (int)lattice_l, (int)layers_left, digit_bits));
+  CUDA_TRY(cudaGetLastError());
+  PPVM_TRY(sync_state(s, 0));
+  if (s->h_ctrl->err) {
+    s->poisoned = true;
+    return fail(PPVM_ECUDA, "device error in budget truncation");
+  }
+  s->n_host = s->h_ctrl->n;
+  s->n_ub = s->n_host;
   return PPVM_OK;
 }
 

@@ -302,13 +302,21 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
   __shared__ unsigned long long s_created[kRunMaxGates];
+  __shared__ double s_cs[kRunMaxGates], s_sn[kRunMaxGates];
+  __shared__ uint16_t s_gidx[64 * W];               // qubit -> its gate's index in the run
+  __shared__ uint8_t s_ord[kRunWarps][kRunMaxK];    // a group's coordinate bits in gate order
   if (ld_volatile_int(&ctrl->err)) return;
   const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs);
   const unsigned long long ubase = ld_volatile(&ctrl->n_s);  // untouched survivors go first
   const uint32_t cls = rd->cls;
   const uint32_t L = rd->L;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (unsigned j = threadIdx.x; j < L; j += blockDim.x) s_created[j] = 0;
+  for (unsigned j = threadIdx.x; j < L; j += blockDim.x) {
+    s_created[j] = 0;
+    s_cs[j] = rd->cs[j];
+    s_sn[j] = rd->sn[j];
+    s_gidx[rd->q[j]] = (uint16_t)j;  // the qubits of a run are distinct
+  }
   __syncthreads();
   const unsigned long long ntiles = (ngroups + kRunWarps - 1) / kRunWarps;
   const bool wcap = maxw != ~0ull;
@@ -343,6 +351,16 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
         }
       }
       size = 1u << k;
+      if (lane == 0) {  // coordinate bits sorted by the position of their gate in the run
+        for (unsigned t = 0; t < k; ++t) {
+          unsigned r = t;
+          while (r > 0 && s_gidx[pos[s_ord[warp][r - 1]]] > s_gidx[pos[t]]) {
+            s_ord[warp][r] = s_ord[warp][r - 1];
+            --r;
+          }
+          s_ord[warp][r] = (uint8_t)t;
+        }
+      }
       if (wcap) {
         unsigned wt = 0;
 #pragma unroll
@@ -369,13 +387,11 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
       //   RX: eps = b ? -1 : +1   (crates/ppvm-pauli-sum/src/sum/rot1.rs:73)
       //   RZ: eps = b ? +1 : -1   (rot1.rs:124)
       const double eps_a = cls == 0 ? 1.0 : -1.0, eps_b = -eps_a;
-      for (uint32_t j = 0; j < L; ++j) {
-        const unsigned q = rd->q[j];
-        if (!((M[q >> 6] >> (q & 63)) & 1ull)) continue;
-        unsigned t = 0;
-        while (pos[t] != q) ++t;
+      for (unsigned r = 0; r < k; ++r) {  // the group's gates, in run order
+        const unsigned t = s_ord[warp][r];
+        const unsigned j = s_gidx[pos[t]];
         const unsigned bit = 1u << t;
-        const double cs = rd->cs[j], sn = rd->sn[j];
+        const double cs = s_cs[j], sn = s_sn[j];
         unsigned made = 0;
         for (unsigned p = lane; p < size / 2; p += 32) {
           const unsigned a = ((p >> t) << (t + 1)) | (p & (bit - 1));
@@ -474,27 +490,52 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
 }
 
 // Publishes the count after the run and fills the op log of its gates (and its TRUNCATE).
-static __global__ void k_run_commit(Ctrl* ctrl, RunScratch R, int op0, int L, int trunc_op, OpLog* log) {
-  for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
-  if (ctrl->err) return;
-  const unsigned long long n0 = ctrl->n;
-  const unsigned long long ngroups = ctrl->n_pairs;
-  unsigned long long n = n0;
-  for (int j = 0; j < L; ++j) {
-    log[op0 + j].n_in = n;
-    log[op0 + j].n_new = R.created[j];
-    n += R.created[j];
-    log[op0 + j].n_out = n;
+// One block of kRunMaxGates threads: thread j logs gate j (an inclusive scan of the created
+// counts gives each gate's live count).
+static __global__ void __launch_bounds__(kRunMaxGates) k_run_commit(Ctrl* ctrl, RunScratch R, int op0, int L,
+                                                                    int trunc_op, OpLog* log) {
+  __shared__ unsigned long long s_w[kRunMaxGates / 32];
+  __shared__ int s_err;
+  if (threadIdx.x == 0) s_err = ctrl->err;
+  __syncthreads();
+  if (s_err) {
+    if (threadIdx.x < 4) ctrl->tickets[threadIdx.x] = 0;
+    return;
+  }
+  const unsigned long long n0 = ctrl->n, ngroups = ctrl->n_pairs;
+  const int j = threadIdx.x, lane = j & 31, warp = j >> 5;
+  const unsigned long long mine = j < L ? R.created[j] : 0ull;
+  unsigned long long incl = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_w[warp] = incl;
+  __syncthreads();
+  unsigned long long before = 0;
+  for (int w = 0; w < warp; ++w) before += s_w[w];
+  incl += before;
+  unsigned long long total = 0;
+  for (int w = 0; w < kRunMaxGates / 32; ++w) total += s_w[w];
+  if (j < L) {
+    log[op0 + j].n_in = n0 + incl - mine;
+    log[op0 + j].n_new = mine;
+    log[op0 + j].n_out = n0 + incl;
     log[op0 + j].n_s = 0;
   }
-  log[op0].n_s = ctrl->n_side;                               // touched terms (profiling bytes)
-  if (L > 1) log[op0 + L - 1].n_s = (ngroups == 0) ? 0 : ctrl->cap_needed - ctrl->n_s;  // group outputs
-  const unsigned long long out = (ngroups == 0) ? ctrl->n_s : ctrl->cap_needed;
-  if (trunc_op >= 0) {
-    log[trunc_op].n_in = n;
-    log[trunc_op].n_out = out;
+  __syncthreads();
+  if (j == 0) {
+    for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
+    log[op0].n_s = ctrl->n_side;  // touched terms (profiling bytes)
+    if (L > 1) log[op0 + L - 1].n_s = (ngroups == 0) ? 0 : ctrl->cap_needed - ctrl->n_s;  // group outputs
+    const unsigned long long out = (ngroups == 0) ? ctrl->n_s : ctrl->cap_needed;
+    if (trunc_op >= 0) {
+      log[trunc_op].n_in = n0 + total;
+      log[trunc_op].n_out = out;
+    }
+    ctrl->n = out;
   }
-  ctrl->n = out;
 }
 
 }  // namespace ppvm

@@ -340,6 +340,24 @@ class PauliSum:
         gl = ops if isinstance(ops, GateList) else ops_array(ops)
         self._check(lib().ppvm_gate_list_run(self._h, gl.ptr, len(gl)))
 
+    def truncate_budget(self, budget: int, net=None, lattice: int = 0, layers_left: int = 0,
+                        digit_bits: int = 8) -> None:
+        """Keeps the ``budget`` terms of highest priority, in order: |c| (``net`` None) or the
+        score of a ``TermPriorityNet`` (ppvm_b200.learned) on an ``lattice`` x ``lattice`` grid
+        with ``layers_left`` layers still to apply."""
+        self._check(lib().ppvm_truncate_budget(self._h, int(budget), net._h if net is not None else None,
+                                               int(lattice), int(layers_left), int(digit_bits)))
+
+    def features(self, lattice: int, layers_left: int) -> np.ndarray:
+        """Per-term features of learned truncation, ``[len(self), 8]`` float32, iteration order."""
+        n = len(self)
+        out = np.zeros((max(n, 1), 8), dtype=np.float32)
+        got = ctypes.c_size_t()
+        self._check(lib().ppvm_term_features(self._h, int(lattice), int(layers_left),
+                                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n,
+                                             ctypes.byref(got)))
+        return out[: got.value]
+
     def launch_count(self) -> int:
         """Kernels this sum has launched since it was created."""
         n = ctypes.c_uint64()

@@ -1,0 +1,103 @@
+"""GPU tests of learned truncation: the tensor-core network against the FP64 CPU reference
+(oracle/mlp_ref.py), its training, and term-budget truncation against a host selection."""
+
+import numpy as np
+import pytest
+
+from oracle import mlp_ref as M
+from ppvm_b200 import circuits as C
+from ppvm_b200.learned import TermPriorityNet, split_layers
+from ppvm_b200.paulisum import PauliSum
+
+pytestmark = pytest.mark.gpu
+
+
+def rand_net(seed):
+    rng = np.random.default_rng(seed)
+    net = TermPriorityNet(seed=seed)
+    p = M.unpack(rng.normal(0, 1, M.N_PARAMS))
+    p["W1"] *= 0.35
+    p["W2"] *= 0.125
+    p["w3"] *= 0.125
+    p["b1"] *= 0.1
+    p["b2"] *= 0.1
+    net.params = M.pack(p).astype(np.float32)
+    return net, rng
+
+
+def test_forward_matches_reference():
+    net, rng = rand_net(1)
+    X = rng.normal(0, 1, (1000, 8)).astype(np.float32)
+    y = net.predict(X)
+    want, _ = M.forward(net.params.astype(np.float64), X, tc=True)
+    assert np.max(np.abs(y - want) / (1 + np.abs(want))) < 1e-2
+    exact, _ = M.forward(net.params.astype(np.float64), X, tc=False)
+    assert np.max(np.abs(y - exact) / (1 + np.abs(exact))) < 5e-2
+
+
+def test_gradient_matches_reference():
+    net, rng = rand_net(2)
+    X = rng.normal(0, 1, (2000, 8)).astype(np.float32)
+    t = rng.normal(0, 1, 2000).astype(np.float32)
+    g, loss = net.grad(X, t)
+    want_loss, want = M.loss_and_grad(net.params.astype(np.float64), X, t, tc=True)
+    assert abs(loss - want_loss) < 1e-2 * (1 + want_loss)
+    rel = np.linalg.norm(g - want) / np.linalg.norm(want)
+    cos = float(g @ want / (np.linalg.norm(g) * np.linalg.norm(want)))
+    assert rel < 5e-2 and cos > 0.998, (rel, cos)
+    for name, sl in (("W1", slice(0, 512)), ("W2", slice(576, 4672)), ("w3", slice(4736, 4800))):
+        r = np.linalg.norm(g[sl] - want[sl]) / np.linalg.norm(want[sl])
+        assert r < 6e-2, (name, r)
+
+
+def test_training_fits_a_smooth_target():
+    net, rng = rand_net(3)
+    X = rng.uniform(-1, 1, (20000, 8)).astype(np.float32)
+    t = (np.sin(2 * X[:, 0]) + X[:, 1] * X[:, 2] - 0.5 * X[:, 3] ** 2).astype(np.float32)
+    before = float(np.mean((net.predict(X) - t) ** 2))
+    net.train(X, t, epochs=30, batch=512, lr=3e-3, seed=1)
+    after = float(np.mean((net.predict(X) - t) ** 2))
+    assert after < 0.05 * before and after < 0.02, (before, after)
+
+
+def _sum_after(L=5, layers=3):
+    wl = C.kicked_ising_random_h(L=L, layers=layers, seed=5, thr=1e-7, obs=(L // 2, L // 2))
+    s = PauliSum([wl.observable[0][0]], wl.n_qubits, [1.0], min_abs_coeff=1e-7, clifford_angles=True)
+    for part in split_layers(wl.ops)[:layers]:
+        s.run(part)
+    return s
+
+
+def _expected_kept(keys, B):
+    order = np.lexsort((np.arange(len(keys)), -keys.astype(np.int64)))  # by key desc, then index
+    return np.sort(order[:B])
+
+
+@pytest.mark.parametrize("bits", [8, 11])
+def test_budget_truncation_plain_keeps_the_top_by_magnitude(bits):
+    s = _sum_after()
+    terms = s.terms
+    n = len(terms)
+    assert n > 3000
+    c = np.array([abs(v) for _, v in terms])
+    keys = (c.view(np.uint64) >> np.uint64(32)).astype(np.uint64)
+    for B in (n // 3, 1000, 1):
+        t = _sum_after()
+        t.truncate_budget(B, digit_bits=bits)
+        kept = _expected_kept(keys, B)
+        assert t.terms == [terms[i] for i in kept]
+
+
+def test_budget_truncation_learned_keeps_the_top_scores():
+    net, _ = rand_net(4)
+    s = _sum_after()
+    terms = s.terms
+    f = s.features(5, 2)
+    score = net.predict(f)
+    u = score.view(np.uint32).astype(np.uint64)
+    keys = np.where(u & 0x80000000, (~u) & 0xFFFFFFFF, u | 0x80000000)
+    B = len(terms) // 4
+    s.truncate_budget(B, net, 5, 2)
+    assert s.terms == [terms[i] for i in _expected_kept(keys, B)]
+    s.truncate_budget(10 ** 9, net, 5, 2)  # larger than the sum: nothing changes
+    assert len(s) == B
