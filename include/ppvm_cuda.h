@@ -289,6 +289,13 @@ ppvm_status ppvm_batch_term_gate_updates(const ppvm_batch* batch, uint64_t* per_
 /* Bytes this batch has copied host->device and device->host since it was created. */
 ppvm_status ppvm_batch_transfer_counters(const ppvm_batch* batch, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
+/* ---- memory -------------------------------------------------------------------------- */
+/* The large buffers of a sum (term planes, scratch) come from a per-device cache: a
+ * destroyed or grown sum gives them back to the cache, and later sums reuse them without
+ * cudaMalloc/cudaFree (which synchronise the device).  This call returns every cached buffer
+ * to the driver.  No counterpart in the reference (Rust's allocator plays this part). */
+ppvm_status ppvm_release_cached_memory(void);
+
 /* ---- diagnostics ------------------------------------------------------------------- */
 /* Thread-local text of the last failing call ("" if none). */
 const char* ppvm_last_error_string(void);

@@ -104,6 +104,7 @@ _SIGS = {
     "ppvm_batch_export_terms": [_P, _SZ, _U64P, _U64P, _DP, _SZ, _SZP],
     "ppvm_batch_term_gate_updates": [_P, _U64P, _U64P],
     "ppvm_batch_transfer_counters": [_P, _U64P, _U64P],
+    "ppvm_release_cached_memory": [],
     "ppvm_profile_enable": [_P, _I],
     "ppvm_profile_read": [_P, ctypes.c_char_p, _SZ, _DP, _U64P, _U64P, _SZ, _SZP],
 }

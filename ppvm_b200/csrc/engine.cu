@@ -10,7 +10,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <set>
+#include <unordered_map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -196,6 +199,57 @@ struct ppvm_sum {
 
 namespace {
 
+// ---- caching pool for the large per-sum buffers -----------------------------------------------
+// Term planes and scratch are taken from, and given back to, a per-device free list instead of
+// cudaMalloc/cudaFree on every sum: creating sums of the same size again (a user's loop over
+// circuits, the term-budget runs of learned truncation) then allocates nothing and does not
+// synchronise the device.  Buffers are handed back only when their sum's stream is idle.
+// ppvm_release_cached_memory() returns the cached memory to the driver.
+std::mutex g_pool_mu;
+std::multimap<size_t, void*> g_pool_free[64];
+std::unordered_map<void*, std::pair<int, size_t>> g_pool_live;
+
+void pool_release_device(int dev) {  // caller holds g_pool_mu; dev is current
+  for (auto& kv : g_pool_free[dev]) cudaFree(kv.second);
+  g_pool_free[dev].clear();
+}
+
+cudaError_t pool_malloc(void** out, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaMalloc(out, bytes);
+  const size_t want = (bytes + ((1u << 20) - 1)) & ~(size_t)((1u << 20) - 1);  // 1 MiB granules
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pool_free[dev].lower_bound(want);
+  if (it != g_pool_free[dev].end() && it->first <= want + want / 2) {
+    *out = it->second;
+    g_pool_live[it->second] = {dev, it->first};
+    g_pool_free[dev].erase(it);
+    return cudaSuccess;
+  }
+  e = cudaMalloc(out, want);
+  if (e == cudaErrorMemoryAllocation) {  // give the cache back and try once more
+    cudaGetLastError();
+    pool_release_device(dev);
+    e = cudaMalloc(out, want);
+  }
+  if (e == cudaSuccess) g_pool_live[*out] = {dev, want};
+  return e;
+}
+
+void pool_free(void* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pool_live.find(p);
+  if (it == g_pool_live.end()) {
+    cudaFree(p);
+    return;
+  }
+  g_pool_free[it->second.first].emplace(it->second.second, p);
+  g_pool_live.erase(it);
+}
+
 unsigned long long next_pow2(unsigned long long v) {
   unsigned long long p = 1;
   while (p < v) p <<= 1;
@@ -214,20 +268,20 @@ ppvm_status ensure_device(int dev) {
 }
 
 void free_scratch(ppvm_sum* s) {
-  cudaFree(s->alt);
-  cudaFree(s->tstate2);
+  pool_free(s->alt);
+  pool_free(s->tstate2);
   uint32_t* run_arrays[] = {s->R.gslot, s->R.grp_min, s->R.grp_cnt, s->R.grp_ord, s->R.g_start,
                             s->R.g_cnt, s->R.g_rep, s->R.g_fill, s->R.members};
-  for (uint32_t* p : run_arrays) cudaFree(p);
-  cudaFree(s->R.created);
+  for (uint32_t* p : run_arrays) pool_free(p);
+  pool_free(s->R.created);
   s->R = RunScratch{};
   s->alt = nullptr;
   s->tstate2 = nullptr;
-  cudaFree(s->s_idx);
-  cudaFree(s->s_rec);
-  cudaFree(s->partner);
-  cudaFree(s->table);
-  cudaFree(s->tstate);
+  pool_free(s->s_idx);
+  pool_free(s->s_rec);
+  pool_free(s->partner);
+  pool_free(s->table);
+  pool_free(s->tstate);
   s->s_idx = nullptr;
   s->s_rec = nullptr;
   s->partner = nullptr;
@@ -240,42 +294,42 @@ ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   if (new_cap >= 0xFFFFFFF0ull) return fail(PPVM_ECAPACITY, "term capacity limit (2^32) exceeded");
   const int W = s->W;
   uint64_t* np = nullptr;
-  CUDA_TRY(cudaMalloc(&np, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&np, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
   if (s->planes) {
     for (int w = 0; w < 2 * W + 1; ++w)
       CUDA_TRY(cudaMemcpyAsync(np + (size_t)w * new_cap, s->planes + (size_t)w * s->cap,
                                sizeof(uint64_t) * s->n_host, cudaMemcpyDeviceToDevice, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
-    cudaFree(s->planes);
+    pool_free(s->planes);
   }
   s->planes = np;
   s->cap = new_cap;
   free_scratch(s);
-  CUDA_TRY(cudaMalloc(&s->s_idx, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->partner, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->s_rec, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->s_idx, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->partner, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->s_rec, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
   s->table_cap = next_pow2(std::max<unsigned long long>(2 * new_cap, 1024));
-  CUDA_TRY(cudaMalloc(&s->table, sizeof(unsigned long long) * s->table_cap));
+  CUDA_TRY(pool_malloc((void**)&s->table, sizeof(unsigned long long) * s->table_cap));
   CUDA_TRY(cudaMemsetAsync(s->table, 0, sizeof(unsigned long long) * s->table_cap, s->stream));
   s->table_epoch = 0;
   // one tile-state word per look-back tile: the smallest tile is k_run_groups' kRunWarps groups
   s->tstate_cap = new_cap / kRunWarps + 64;
-  CUDA_TRY(cudaMalloc(&s->tstate, sizeof(unsigned long long) * s->tstate_cap));
+  CUDA_TRY(pool_malloc((void**)&s->tstate, sizeof(unsigned long long) * s->tstate_cap));
   CUDA_TRY(cudaMemsetAsync(s->tstate, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
-  CUDA_TRY(cudaMalloc(&s->tstate2, sizeof(unsigned long long) * s->tstate_cap));
+  CUDA_TRY(pool_malloc((void**)&s->tstate2, sizeof(unsigned long long) * s->tstate_cap));
   CUDA_TRY(cudaMemsetAsync(s->tstate2, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
   s->tile_epoch = 0;
-  CUDA_TRY(cudaMalloc(&s->alt, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->R.gslot, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->R.grp_min, sizeof(uint32_t) * s->table_cap));
-  CUDA_TRY(cudaMalloc(&s->R.grp_cnt, sizeof(uint32_t) * s->table_cap));
-  CUDA_TRY(cudaMalloc(&s->R.grp_ord, sizeof(uint32_t) * s->table_cap));
-  CUDA_TRY(cudaMalloc(&s->R.g_start, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->R.g_cnt, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->R.g_rep, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->R.g_fill, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->R.members, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(cudaMalloc(&s->R.created, sizeof(unsigned long long) * kRunMaxGates));
+  CUDA_TRY(pool_malloc((void**)&s->alt, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.gslot, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.grp_min, sizeof(uint32_t) * s->table_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.grp_cnt, sizeof(uint32_t) * s->table_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.grp_ord, sizeof(uint32_t) * s->table_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.g_start, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.g_cnt, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.g_rep, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.g_fill, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.members, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.created, sizeof(unsigned long long) * kRunMaxGates));
   return PPVM_OK;
 }
 
@@ -1179,7 +1233,7 @@ ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
     cudaFreeHost(ch.h);
     cudaFree(ch.d);
   }
-  cudaFree(s->planes);
+  pool_free(s->planes);
   free_scratch(s);
   cudaFree(s->side);
   cudaFree(s->d_ctrl);
@@ -1715,6 +1769,18 @@ ppvm_status ppvm_truncate_budget(ppvm_sum* s, uint64_t budget, const ppvm_mlp* m
   }
   s->n_host = s->h_ctrl->n;
   s->n_ub = s->n_host;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_release_cached_memory(void) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (int d = 0; d < 64; ++d) {
+    if (g_pool_free[d].empty()) continue;
+    if (cudaSetDevice(d) == cudaSuccess) pool_release_device(d);
+  }
+  cudaSetDevice(cur);
   return PPVM_OK;
 }
 

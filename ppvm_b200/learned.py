@@ -201,7 +201,7 @@ def compare_budgets(L: int = 10, layers: int = 4, seed: int = 2,
     return {"reference": {"O": ref, "s": t_ref, "peak": ref_peak}, "rows": rows,
             "train": {"pairs": int(len(y)), "data_s": t_data, "train_s": t_train, "loss": loss,
                       "label_var": float(np.var(y))},
-            "time_to_tol": {"plain": first_ok("plain"), "learned": first_ok("learned"), "tol": tol}}
+            "time_to_tol": {"plain": first_ok("plain"), "learned": first_ok("learned"), "tol": tol}, "net": net}
 
 
 __all__ = ["TermPriorityNet", "make_training_set", "run_with_budget", "split_layers", "N_PARAMS"]

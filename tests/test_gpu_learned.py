@@ -101,3 +101,26 @@ def test_budget_truncation_learned_keeps_the_top_scores():
     assert s.terms == [terms[i] for i in _expected_kept(keys, B)]
     s.truncate_budget(10 ** 9, net, 5, 2)  # larger than the sum: nothing changes
     assert len(s) == B
+
+
+def test_trained_network_beats_plain_budget_truncation():
+    """What the trained network gains: at matched term budgets the learned priority gives a
+    smaller <O> error than |c| on a circuit the network never saw (10x10, seeded angles;
+    trained on 6x6 circuits with other angles).  The budgets bind between layers 2 and 3."""
+    from ppvm_b200 import learned
+
+    X, y = learned.make_training_set(L=6, layers=4, seeds=(11, 12, 13, 14, 15, 16, 17, 18), per_layer=2048,
+                                     label_thr=1e-5)
+    net = TermPriorityNet(seed=7)
+    net.train(X, y, epochs=300, batch=512, lr=2e-3, seed=3)
+    wl = C.kicked_ising_random_h(L=10, layers=4, seed=2, thr=1e-7)
+    ref, _ = learned.run_with_budget(wl, None)
+    errs = {"plain": [], "learned": []}
+    for B in (2000, 4000, 8000):
+        for kind, nn in (("plain", None), ("learned", net)):
+            v, _ = learned.run_with_budget(wl, B, nn, 10)
+            errs[kind].append(max(abs(v - ref), 1e-12))
+    gp = float(np.exp(np.mean(np.log(errs["plain"]))))
+    gl = float(np.exp(np.mean(np.log(errs["learned"]))))
+    print("geometric-mean |err|: plain", gp, "learned", gl, errs)
+    assert gl < 0.5 * gp, (gl, gp, errs)

@@ -324,3 +324,21 @@ def test_empty_and_edge_cases():
     gx, gz = G.parse_word("XY", 2)
     o.pauli_rotation(gx, gz, 0.4)
     same(s, o)
+
+
+def test_cached_buffers_are_reused_safely():
+    # sums created after others were destroyed take their buffers from the cache: results
+    # stay identical, also after the cache is handed back to the driver
+    from ppvm_b200._lib import lib
+
+    wl = C.kicked_ising_2d(layers=3)
+    got = []
+    for rep in range(3):
+        g = gpu_from(wl.observable, wl.n_qubits, wl.min_abs_coeff, wl.max_weight, True, exact=False)
+        g.run(wl.ops)
+        got.append(_sorted(*g.export()))
+        del g
+        if rep == 1:
+            assert lib().ppvm_release_cached_memory() == 0
+    for k, c in got[1:]:
+        assert np.array_equal(k, got[0][0]) and np.array_equal(c.view(np.uint64), got[0][1].view(np.uint64))
