@@ -271,6 +271,11 @@ ppvm_status ppvm_batch_set_ops(ppvm_batch* batch, size_t inst, const ppvm_op* op
 ppvm_status ppvm_batch_run(ppvm_batch* batch);
 /* The same in one launch: each CTA runs its instance's whole list. */
 ppvm_status ppvm_batch_run_persistent(ppvm_batch* batch);
+/* Term capacity per instance (n_inst values): reserve raises capacities before a run (a
+ * caller that knows the peak sizes avoids the growth replays of a first run); get reads the
+ * current ones (after a run: at least each instance's peak). */
+ppvm_status ppvm_batch_reserve(ppvm_batch* batch, const uint64_t* caps);
+ppvm_status ppvm_batch_get_capacity(const ppvm_batch* batch, uint64_t* caps);
 /* Launch configuration: CTA size (128, 256, 512), items per thread (2, 4) and pair-table
  * slots per term of capacity (2, 4).  ppvm_batch_autotune times every combination on this
  * batch (a full run each) and keeps the fastest; best_ms = its run time. */

@@ -96,6 +96,8 @@ _SIGS = {
     "ppvm_batch_set_ops": [_P, _SZ, ctypes.POINTER(Op), _SZ],
     "ppvm_batch_run": [_P],
     "ppvm_batch_run_persistent": [_P],
+    "ppvm_batch_reserve": [_P, _U64P],
+    "ppvm_batch_get_capacity": [_P, _U64P],
     "ppvm_batch_set_config": [_P, _I, _I, _I],
     "ppvm_batch_get_config": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "ppvm_batch_autotune": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), _DP],

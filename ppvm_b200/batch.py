@@ -18,20 +18,21 @@ import numpy as np
 
 from . import gates as G
 from ._lib import EINVAL, FLAG_CLIFFORD_ANGLES, OK, UMAX, PPVMError, lib
-from .paulisum import _p64, _pd, ops_array
+from .paulisum import GateList, _p64, _pd, ops_array
 
 
 @dataclass
 class Instance:
     n_qubits: int
     terms: list  # [(word, coeff)]
-    ops: list    # gate tuples
+    ops: list    # gate tuples, or a GateList packed once with ops_array
     min_abs_coeff: float = 1e-10
     max_pauli_weight: int | None = None
 
 
 class PauliSumBatch:
-    def __init__(self, instances: list[Instance], *, clifford_angles: bool = False, device: int = 0):
+    def __init__(self, instances: list[Instance], *, clifford_angles: bool = False, device: int = 0,
+                 capacity=None):
         if not instances:
             raise ValueError("a batch needs at least one instance")
         k = len(instances)
@@ -54,8 +55,13 @@ class PauliSumBatch:
                     x[t], z[t] = G.parse_word(w, inst.n_qubits)
                 c = np.array([float(cf) for _, cf in inst.terms], dtype=np.float64)
                 self._check(lib().ppvm_batch_add_terms(self._h, j, _p64(x), _p64(z), _pd(c), len(c)))
-            gl = ops_array(inst.ops)
+            gl = inst.ops if isinstance(inst.ops, GateList) else ops_array(inst.ops)
             self._check(lib().ppvm_batch_set_ops(self._h, j, gl.ptr, len(gl)))
+        if capacity is not None:
+            caps = np.ascontiguousarray(capacity, dtype=np.uint64)
+            if caps.shape != (k,):
+                raise ValueError("capacity needs one value per instance")
+            self._check(lib().ppvm_batch_reserve(self._h, _p64(caps)))
 
     @classmethod
     def from_workloads(cls, workloads, **kw) -> "PauliSumBatch":
@@ -86,6 +92,12 @@ class PauliSumBatch:
     def run_persistent(self) -> None:
         """The same in one launch (each CTA runs its instance's whole list)."""
         self._check(lib().ppvm_batch_run_persistent(self._h))
+
+    def capacities(self) -> np.ndarray:
+        """Term capacity of every instance (after a run: at least its peak live count)."""
+        caps = np.zeros(len(self), dtype=np.uint64)
+        self._check(lib().ppvm_batch_get_capacity(self._h, _p64(caps)))
+        return caps
 
     def set_config(self, block: int, items: int, table_factor: int) -> None:
         self._check(lib().ppvm_batch_set_config(self._h, block, items, table_factor))

@@ -1032,6 +1032,24 @@ ppvm_status ppvm_batch_set_ops(ppvm_batch* b, size_t inst, const ppvm_op* ops, s
   return PPVM_OK;
 }
 
+ppvm_status ppvm_batch_reserve(ppvm_batch* b, const uint64_t* caps) {
+  if (!b || !caps) return bfail(PPVM_EINVAL, "null argument");
+  for (size_t i = 0; i < b->ninst; ++i) {
+    if (caps[i] >= 0xFFFFFFF0ull) return bfail(PPVM_EINVAL, "capacity limit (2^32) exceeded");
+    if (caps[i] > b->cap[i]) {
+      b->cap[i] = caps[i];
+      b->layout_dirty = true;
+    }
+  }
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_get_capacity(const ppvm_batch* b, uint64_t* caps) {
+  if (!b || !caps) return bfail(PPVM_EINVAL, "null argument");
+  for (size_t i = 0; i < b->ninst; ++i) caps[i] = b->cap[i];
+  return PPVM_OK;
+}
+
 ppvm_status ppvm_batch_set_config(ppvm_batch* b, int block, int items, int table_factor) {
   if (!b) return bfail(PPVM_EINVAL, "null batch");
   if ((block != 128 && block != 256 && block != 512) || (items != 2 && items != 4) ||

@@ -250,6 +250,9 @@ void pool_free(void* p) {
   g_pool_live.erase(it);
 }
 
+void destroy_now(ppvm_sum* s);                 // frees a sum and everything it holds
+ppvm_sum* take_cached(int device, int W);      // a cached sum of that device and width, or null
+
 unsigned long long next_pow2(unsigned long long v) {
   unsigned long long p = 1;
   while (p < v) p <<= 1;
@@ -1181,15 +1184,45 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
   if (n_qubits == 0 || n_qubits > 64 * kMaxW)
     return fail(PPVM_EINVAL, "n_qubits must be in [1, 512]");
   PPVM_TRY(ensure_device(device));
+  const int W = (int)((n_qubits + 63) / 64);
+  if (ppvm_sum* c = take_cached(device, W)) {  // a cached handle: reset its state
+    c->n = n_qubits;
+    c->thr = min_abs_coeff;
+    c->maxw = max_weight;
+    c->flags = flags;
+    c->n_host = c->n_ub = 0;
+    c->poisoned = false;
+    c->swaps.clear();
+    c->no_fuse.clear();
+    c->npres = 0;
+    c->h_pres.clear();
+    c->prof = false;
+    for (int f = 0; f < F_COUNT; ++f) c->prof_ms[f] = 0, c->prof_launches[f] = 0, c->prof_bytes[f] = 0;
+    c->launch_count = c->xfer_h2d = c->xfer_d2h = 0;
+    c->last_nops = 0;
+    std::memset(c->h_ctrl, 0, sizeof(Ctrl));
+    ppvm_status st = PPVM_OK;
+    if (cudaMemsetAsync(c->d_ctrl, 0, sizeof(Ctrl), c->stream) != cudaSuccess)
+      st = fail(PPVM_ECUDA, "memset failed");
+    if (st == PPVM_OK && c->cap < std::max<size_t>(capacity_hint, 4096))
+      st = grow(c, std::max<size_t>(capacity_hint, 4096));
+    if (st == PPVM_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) st = fail(PPVM_ECUDA, "sync failed");
+    if (st != PPVM_OK) {
+      destroy_now(c);
+      return st;
+    }
+    *out = c;
+    return PPVM_OK;
+  }
   ppvm_sum* s = new ppvm_sum();
   s->device = device;
   s->n = n_qubits;
-  s->W = (int)((n_qubits + 63) / 64);
+  s->W = W;
   s->thr = min_abs_coeff;
   s->maxw = max_weight;
   s->flags = flags;
   auto bail = [&](ppvm_status st) {
-    ppvm_sum_destroy(s);
+    destroy_now(s);
     return st;
   };
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -1220,8 +1253,16 @@ ppvm_status ppvm_sum_create(ppvm_sum** out, uint32_t n_qubits, double min_abs_co
   return ppvm_sum_create2(out, n_qubits, min_abs_coeff, max_weight, capacity_hint, 0, 0);
 }
 
-ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
-  if (!s) return PPVM_OK;
+}  // extern "C"
+
+namespace {
+// Destroyed sums that own their stream go to a small per-process cache and are handed out
+// again by ppvm_sum_create2 for the same device and plane width, with every buffer, the
+// stream and the upload arena still allocated: creating a sum then costs no allocation.
+std::vector<ppvm_sum*> g_sum_cache;  // guarded by g_pool_mu
+constexpr size_t kSumCacheMax = 8;
+
+void destroy_now(ppvm_sum* s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (auto& L : s->prof_pending) {
@@ -1249,6 +1290,52 @@ ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
   cudaFree(s->d_pres_table);
   if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
   delete s;
+}
+
+ppvm_sum* take_cached(int device, int W) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (size_t i = 0; i < g_sum_cache.size(); ++i)
+    if (g_sum_cache[i]->device == device && g_sum_cache[i]->W == W) {
+      ppvm_sum* s = g_sum_cache[i];
+      g_sum_cache.erase(g_sum_cache.begin() + (long)i);
+      return s;
+    }
+  return nullptr;
+}
+}  // namespace
+
+extern "C" {
+
+ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
+  if (!s) return PPVM_OK;
+  cudaSetDevice(s->device);
+  const bool idle = !s->stream || cudaStreamSynchronize(s->stream) == cudaSuccess;
+  if (idle && !s->poisoned && !s->own_stream) {  // give a cached handle a stream of its own
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+      s->stream = st;
+      s->own_stream = true;
+    }
+  }
+  if (idle && !s->poisoned && s->own_stream) {
+    for (auto& L : s->prof_pending) {
+      s->event_pool.push_back(L.a);
+      s->event_pool.push_back(L.b);
+    }
+    s->prof_pending.clear();
+    cudaFree(s->d_pat);
+    cudaFree(s->d_pres_keys);
+    cudaFree(s->d_pres_table);
+    s->d_pat = nullptr;
+    s->d_pres_keys = nullptr;
+    s->d_pres_table = nullptr;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (g_sum_cache.size() < kSumCacheMax) {
+      g_sum_cache.push_back(s);
+      return PPVM_OK;
+    }
+  }
+  destroy_now(s);
   return PPVM_OK;
 }
 
@@ -1317,14 +1404,17 @@ ppvm_status ppvm_sum_add_terms(ppvm_sum* s, const uint64_t* x, const uint64_t* z
   }
   PPVM_TRY(ensure_device(s->device));
   if (s->n_host + k > s->cap) PPVM_TRY(grow(s, std::max<unsigned long long>(2 * s->cap, s->n_host + k + 1024)));
-  uint64_t* dx = nullptr;
-  CUDA_TRY(cudaMalloc(&dx, sizeof(uint64_t) * (2 * W + 1) * k));
-  uint64_t* dz = dx + W * k;
-  double* dc = reinterpret_cast<double*>(dx + 2 * W * k);
-  CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(uint64_t) * W * k, cudaMemcpyHostToDevice, s->stream));
-  CUDA_TRY(cudaMemcpyAsync(dz, z, sizeof(uint64_t) * W * k, cudaMemcpyHostToDevice, s->stream));
-  CUDA_TRY(cudaMemcpyAsync(dc, c, sizeof(double) * k, cudaMemcpyHostToDevice, s->stream));
-  s->xfer_h2d += sizeof(uint64_t) * (2 * W + 1) * k;
+  // the new terms go up through the pinned upload arena (the stream is idle between calls)
+  std::vector<uint64_t> packed((size_t)(2 * W + 1) * k);
+  std::memcpy(packed.data(), x, sizeof(uint64_t) * W * k);
+  std::memcpy(packed.data() + (size_t)W * k, z, sizeof(uint64_t) * W * k);
+  std::memcpy(packed.data() + (size_t)2 * W * k, c, sizeof(double) * k);
+  stage_reset(s);
+  const void* d_packed = nullptr;
+  PPVM_TRY(stage_put(s, packed.data(), sizeof(uint64_t) * packed.size(), &d_packed));
+  const uint64_t* dx = static_cast<const uint64_t*>(d_packed);
+  const uint64_t* dz = dx + (size_t)W * k;
+  const double* dc = reinterpret_cast<const double*>(dx + (size_t)2 * W * k);
   unsigned long long mask;
   unsigned ep;
   ppvm_status st = build_index(s, s->n_host + k, &mask, &ep);
@@ -1332,7 +1422,6 @@ ppvm_status ppvm_sum_add_terms(ppvm_sum* s, const uint64_t* x, const uint64_t* z
     DISPATCH_W(W, add_seq(s, dx, dz, dc, k, mask, ep));
     st = sync_state(s, 0);
   }
-  cudaFree(dx);
   PPVM_TRY(st);
   if (s->h_ctrl->err) {
     s->poisoned = true;
@@ -1775,6 +1864,12 @@ ppvm_status ppvm_truncate_budget(ppvm_sum* s, uint64_t budget, const ppvm_mlp* m
 ppvm_status ppvm_release_cached_memory(void) {
   int cur = 0;
   cudaGetDevice(&cur);
+  std::vector<ppvm_sum*> handles;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    handles.swap(g_sum_cache);
+  }
+  for (ppvm_sum* h : handles) destroy_now(h);  // their buffers go back to the pool first
   std::lock_guard<std::mutex> lk(g_pool_mu);
   for (int d = 0; d < 64; ++d) {
     if (g_pool_free[d].empty()) continue;

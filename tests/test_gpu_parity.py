@@ -342,3 +342,20 @@ def test_cached_buffers_are_reused_safely():
             assert lib().ppvm_release_cached_memory() == 0
     for k, c in got[1:]:
         assert np.array_equal(k, got[0][0]) and np.array_equal(c.view(np.uint64), got[0][1].view(np.uint64))
+
+
+def test_reused_handles_start_clean():
+    # a destroyed sum's handle is handed out again for the same width: nothing of the old sum
+    # (terms, preserve strings, strategy, flags, counters) may leak into the new one
+    a = PauliSum(["ZII", "XXX"], 3, [1e-6, 0.7], min_abs_coeff=0.5, preserve_strings=["ZII"], exact_order=True)
+    a.truncate()
+    assert [w for w, _ in a.terms] == ["XXX", "ZII"]
+    del a
+    for n in (3, 5):
+        b = PauliSum(["Z" + "I" * (n - 1), "X" * n], n, [1e-6, 0.7], min_abs_coeff=0.5)
+        assert len(b) == 2 and b.launch_count() < 10
+        b.truncate()
+        assert [w for w, _ in b.terms] == ["X" * n]
+        del b
+    wl = C.tfim_1d(steps=3)
+    run_both(wl.observable, wl.n_qubits, wl.ops, thr=wl.min_abs_coeff, check_every=40, exact=False)
