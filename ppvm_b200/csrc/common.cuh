@@ -138,6 +138,58 @@ static __device__ unsigned long long lookback(unsigned long long* ts, unsigned t
   return r;
 }
 
+// Exclusive prefix of tile `tile` for a tile owned by one warp (all 32 lanes call it): the
+// warp publishes its aggregate, looks back over its predecessors 32 at a time, then
+// publishes its inclusive prefix.  Bounded like lookback(); no block barrier.
+__device__ __forceinline__ unsigned long long warp_lookback(unsigned long long* ts, unsigned long long tile,
+                                                            unsigned long long agg, unsigned epoch, Ctrl* ctrl,
+                                                            int op) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned ep = epoch & 0xFFFFFu;
+  unsigned long long excl = 0;
+  if (tile == 0) {
+    if (lane == 0) st_release(&ts[0], pack_state(epoch, 2, agg));
+    __syncwarp();
+    return 0;
+  }
+  if (lane == 0) st_release(&ts[tile], pack_state(epoch, 1, agg));
+  long long pred = (long long)tile - 1 - (long long)lane;
+  unsigned spins = 0;
+  while (true) {
+    unsigned flag;
+    unsigned long long val;
+    while (true) {
+      if (pred >= 0) {
+        const unsigned long long st = ld_acquire(&ts[pred]);
+        flag = ((unsigned)(st >> 44) == ep) ? (unsigned)((st >> 42) & 3ull) : 0u;
+        val = st & kValueMask;
+      } else {
+        flag = 2;
+        val = 0;
+      }
+      if (__all_sync(kFull, flag != 0)) break;
+      if (++spins > kSpinLimit) {
+        if (lane == 0) set_err(ctrl, kErrTimeout, op);
+        flag = 2;
+        val = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+    const unsigned pmask = __ballot_sync(kFull, flag == 2);
+    const unsigned first = pmask ? (unsigned)(__ffs(pmask) - 1) : 32u;
+    unsigned long long contrib = (lane <= first) ? val : 0ull;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) contrib += __shfl_down_sync(kFull, contrib, o);
+    excl += __shfl_sync(kFull, contrib, 0);
+    if (pmask) break;
+    pred -= 32;
+  }
+  if (lane == 0) st_release(&ts[tile], pack_state(epoch, 2, excl + agg));
+  __syncwarp();
+  return excl;
+}
+
 // Takes the next tile ticket (all threads get the same value).
 __device__ __forceinline__ unsigned next_tile(unsigned long long* counter, unsigned* s_tile) {
   if (threadIdx.x == 0) *s_tile = (unsigned)atomicAdd(counter, 1ull);

@@ -316,7 +316,7 @@ ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   CUDA_TRY(cudaMemsetAsync(s->table, 0, sizeof(unsigned long long) * s->table_cap, s->stream));
   s->table_epoch = 0;
   // one tile-state word per look-back tile: the smallest tile is k_run_groups' kRunWarps groups
-  s->tstate_cap = new_cap / kRunWarps + 64;
+  s->tstate_cap = new_cap + 64;  // one tile-state word per group of a fused run at most
   CUDA_TRY(pool_malloc((void**)&s->tstate, sizeof(unsigned long long) * s->tstate_cap));
   CUDA_TRY(cudaMemsetAsync(s->tstate, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
   CUDA_TRY(pool_malloc((void**)&s->tstate2, sizeof(unsigned long long) * s->tstate_cap));
@@ -716,7 +716,7 @@ struct K {
     {
       ProfScope ps(s, F_RUN_ORDER, op0, L);
       const unsigned ea = s->next_tile_epoch(), eb = s->next_tile_epoch();
-      k_run_order<kScanBlock, 8><<<grid_for(nub, kScanBlock * 8, 8), kScanBlock, 0, s->stream>>>(
+      k_run_order<kScanBlock, 2><<<grid_for(nub, kScanBlock * 2, 8), kScanBlock, 0, s->stream>>>(
           s->d_ctrl, s->R, s->tstate, s->tstate2, ea, eb, op0);
     }
     {

@@ -51,7 +51,9 @@ __device__ __forceinline__ void load_rec(const uint64_t* rec, unsigned long long
 
 template <int W>
 struct ItemsFor {
-  static constexpr int value = W <= 2 ? 8 : (W <= 4 ? 4 : 2);
+  // terms per thread of a look-back tile: small enough that a sum of 10^5..10^6 terms
+  // spreads over a few tiles per SM (a 256-thread tile holds 256 * ITEMS terms)
+  static constexpr int value = W <= 2 ? 4 : (W <= 4 ? 2 : 1);
 };
 
 // ---------------------------------------------------------------------------------------

@@ -290,7 +290,10 @@ k_run_untouched(Planes P, Planes O, Ctrl* ctrl, RunScratch R, int trunc, double 
   }
 }
 
-// One warp per group: butterfly over the group's coordinates, gates in run order.
+// One warp per group: butterfly over the group's coordinates, gates in run order.  Warps
+// are independent: each takes its next group by ticket, so groups of very different sizes do
+// not hold each other up at block barriers.  The group number is also the look-back tile,
+// which places every group's survivors after those of all lower-numbered groups.
 template <int W>
 __global__ void __launch_bounds__(kRunWarps * 32)
 k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, int trunc, double thr,
@@ -298,19 +301,13 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   constexpr int SZ = 1 << kRunMaxK;
   __shared__ double s_coef[kRunWarps][SZ];
   __shared__ unsigned s_ex[kRunWarps][SZ / 32];
-  __shared__ unsigned s_cnt[kRunWarps + 1];
-  __shared__ unsigned s_tile;
-  __shared__ unsigned long long s_slot;
   __shared__ unsigned long long s_created[kRunMaxGates];
   __shared__ double s_cs[kRunMaxGates], s_sn[kRunMaxGates];
   __shared__ uint16_t s_gidx[64 * W];               // qubit -> its gate's index in the run
   __shared__ uint8_t s_ord[kRunWarps][kRunMaxK];    // a group's coordinate bits in gate order
-  if (ld_volatile_int(&ctrl->err)) return;
-  const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs);
-  const unsigned long long ubase = ld_volatile(&ctrl->n_s);  // untouched survivors go first
-  const uint32_t cls = rd->cls;
+  __shared__ int s_err;
+  if (threadIdx.x == 0) s_err = ld_volatile_int(&ctrl->err);
   const uint32_t L = rd->L;
-  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (unsigned j = threadIdx.x; j < L; j += blockDim.x) {
     s_created[j] = 0;
     s_cs[j] = rd->cs[j];
@@ -318,20 +315,24 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
     s_gidx[rd->q[j]] = (uint16_t)j;  // the qubits of a run are distinct
   }
   __syncthreads();
-  const unsigned long long ntiles = (ngroups + kRunWarps - 1) / kRunWarps;
+  if (s_err) return;
+  const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs);
+  const unsigned long long ubase = ld_volatile(&ctrl->n_s);  // untouched survivors go first
+  const uint32_t cls = rd->cls;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool wcap = maxw != ~0ull;
   double* coef = s_coef[warp];
   unsigned* ex = s_ex[warp];
   for (;;) {
-    const unsigned tile = next_tile(&ctrl->tickets[2], &s_tile);
-    if (tile >= ntiles) break;
-    const unsigned long long g = (unsigned long long)tile * kRunWarps + warp;
-    const bool active = g < ngroups;
+    unsigned long long g = 0;
+    if (lane == 0) g = atomicAdd(&ctrl->tickets[2], 1ull);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= ngroups) break;
     uint64_t v[W], f0[W], M[W];
-    unsigned k = 0, size = 0;
+    unsigned k = 0;
     uint16_t pos[kRunMaxK];  // qubit of coordinate bit t (ascending)
     bool wok = true;
-    if (active) {
+    {
       const uint32_t rep = R.g_rep[g];
       uint64_t x[W], z[W], f[W];
       load_key<W>(P, rep, x, z);
@@ -350,139 +351,134 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
           m &= m - 1;
         }
       }
-      size = 1u << k;
-      if (lane == 0) {  // coordinate bits sorted by the position of their gate in the run
-        for (unsigned t = 0; t < k; ++t) {
-          unsigned r = t;
-          while (r > 0 && s_gidx[pos[s_ord[warp][r - 1]]] > s_gidx[pos[t]]) {
-            s_ord[warp][r] = s_ord[warp][r - 1];
-            --r;
-          }
-          s_ord[warp][r] = (uint8_t)t;
+    }
+    const unsigned size = 1u << k;
+    if (lane == 0) {  // coordinate bits sorted by the position of their gate in the run
+      for (unsigned t = 0; t < k; ++t) {
+        unsigned r = t;
+        while (r > 0 && s_gidx[pos[s_ord[warp][r - 1]]] > s_gidx[pos[t]]) {
+          s_ord[warp][r] = s_ord[warp][r - 1];
+          --r;
         }
-      }
-      if (wcap) {
-        unsigned wt = 0;
-#pragma unroll
-        for (int w = 0; w < W; ++w) wt += __popcll(v[w] | f0[w]);
-        wok = wt <= maxw;  // M is inside v, so every member has this weight
-      }
-      for (unsigned e = lane; e < (size + 31) / 32; e += 32) ex[e] = 0u;
-      __syncwarp();
-      const uint32_t start = R.g_start[g], cnt = R.g_cnt[g];
-      for (uint32_t m = lane; m < cnt; m += 32) {
-        const uint32_t i = R.members[start + m];
-        unsigned c = 0;
-        for (unsigned t = 0; t < k; ++t) {
-          const unsigned q = pos[t];
-          const uint64_t fw = cls == 0 ? P.x[(unsigned long long)(q >> 6) * P.cap + i]
-                                       : P.z[(unsigned long long)(q >> 6) * P.cap + i];
-          c |= (unsigned)((fw >> (q & 63)) & 1ull) << t;
-        }
-        coef[c] = P.c[i];
-        atomicOr(&ex[c >> 5], 1u << (c & 31));
-      }
-      __syncwarp();
-      // gates of the run in order; eps of a member with bit t = b:
-      //   RX: eps = b ? -1 : +1   (crates/ppvm-pauli-sum/src/sum/rot1.rs:73)
-      //   RZ: eps = b ? +1 : -1   (rot1.rs:124)
-      const double eps_a = cls == 0 ? 1.0 : -1.0, eps_b = -eps_a;
-      for (unsigned r = 0; r < k; ++r) {  // the group's gates, in run order
-        const unsigned t = s_ord[warp][r];
-        const unsigned j = s_gidx[pos[t]];
-        const unsigned bit = 1u << t;
-        const double cs = s_cs[j], sn = s_sn[j];
-        unsigned made = 0;
-        for (unsigned p = lane; p < size / 2; p += 32) {
-          const unsigned a = ((p >> t) << (t + 1)) | (p & (bit - 1));
-          const unsigned b = a | bit;
-          const bool ea = (ex[a >> 5] >> (a & 31)) & 1u, eb = (ex[b >> 5] >> (b & 31)) & 1u;
-          if (ea && eb) {
-            const double ca = coef[a], cb = coef[b];
-            coef[a] = __dadd_rn(__dmul_rn(ca, cs), __dmul_rn(cb, eps_b * sn));
-            coef[b] = __dadd_rn(__dmul_rn(cb, cs), __dmul_rn(ca, eps_a * sn));
-          } else if (ea) {
-            const double ca = coef[a];
-            coef[a] = __dmul_rn(ca, cs);
-            coef[b] = __dmul_rn(ca, eps_a * sn);
-            atomicOr(&ex[b >> 5], 1u << (b & 31));
-            ++made;
-          } else if (eb) {
-            const double cb = coef[b];
-            coef[b] = __dmul_rn(cb, cs);
-            coef[a] = __dmul_rn(cb, eps_b * sn);
-            atomicOr(&ex[a >> 5], 1u << (a & 31));
-            ++made;
-          }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int o = 16; o; o >>= 1) made += __shfl_down_sync(kFull, made, o);
-        if (lane == 0 && made) atomicAdd(&s_created[j], (unsigned long long)made);
+        s_ord[warp][r] = (uint8_t)t;
       }
     }
-    // survivors, in coordinate order, counted per warp
+    if (wcap) {
+      unsigned wt = 0;
+#pragma unroll
+      for (int w = 0; w < W; ++w) wt += __popcll(v[w] | f0[w]);
+      wok = wt <= maxw;  // M is inside v, so every member has this weight
+    }
+    for (unsigned e = lane; e < (size + 31) / 32; e += 32) ex[e] = 0u;
+    __syncwarp();
+    const uint32_t start = R.g_start[g], cnt = R.g_cnt[g];
+    for (uint32_t m = lane; m < cnt; m += 32) {
+      const uint32_t i = R.members[start + m];
+      uint64_t fw[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w)
+        fw[w] = (M[w] != 0) ? (cls == 0 ? P.x[(unsigned long long)w * P.cap + i]
+                                        : P.z[(unsigned long long)w * P.cap + i])
+                            : 0ull;
+      unsigned c = 0;
+      for (unsigned t = 0; t < k; ++t) {
+        const unsigned q = pos[t];
+        uint64_t word = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) word = (w == (int)(q >> 6)) ? fw[w] : word;
+        c |= (unsigned)((word >> (q & 63)) & 1ull) << t;
+      }
+      coef[c] = P.c[i];
+      atomicOr(&ex[c >> 5], 1u << (c & 31));
+    }
+    __syncwarp();
+    // gates of the run in order; eps of a member with bit t = b:
+    //   RX: eps = b ? -1 : +1   (crates/ppvm-pauli-sum/src/sum/rot1.rs:73)
+    //   RZ: eps = b ? +1 : -1   (rot1.rs:124)
+    const double eps_a = cls == 0 ? 1.0 : -1.0, eps_b = -eps_a;
+    for (unsigned r = 0; r < k; ++r) {
+      const unsigned t = s_ord[warp][r];
+      const unsigned j = s_gidx[pos[t]];
+      const unsigned bit = 1u << t;
+      const double cs = s_cs[j], sn = s_sn[j];
+      unsigned made = 0;
+      for (unsigned p = lane; p < size / 2; p += 32) {
+        const unsigned a = ((p >> t) << (t + 1)) | (p & (bit - 1));
+        const unsigned b = a | bit;
+        const bool ea = (ex[a >> 5] >> (a & 31)) & 1u, eb = (ex[b >> 5] >> (b & 31)) & 1u;
+        if (ea && eb) {
+          const double ca = coef[a], cb = coef[b];
+          coef[a] = __dadd_rn(__dmul_rn(ca, cs), __dmul_rn(cb, eps_b * sn));
+          coef[b] = __dadd_rn(__dmul_rn(cb, cs), __dmul_rn(ca, eps_a * sn));
+        } else if (ea) {
+          const double ca = coef[a];
+          coef[a] = __dmul_rn(ca, cs);
+          coef[b] = __dmul_rn(ca, eps_a * sn);
+          atomicOr(&ex[b >> 5], 1u << (b & 31));
+          ++made;
+        } else if (eb) {
+          const double cb = coef[b];
+          coef[b] = __dmul_rn(cb, cs);
+          coef[a] = __dmul_rn(cb, eps_b * sn);
+          atomicOr(&ex[a >> 5], 1u << (a & 31));
+          ++made;
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int o = 16; o; o >>= 1) made += __shfl_down_sync(kFull, made, o);
+      if (lane == 0 && made) atomicAdd(&s_created[j], (unsigned long long)made);
+    }
+    // survivors, in coordinate order
     unsigned mine = 0;
-    if (active) {
-      for (unsigned c = lane; c < size; c += 32) {
-        const bool e = (ex[c >> 5] >> (c & 31)) & 1u;
-        bool keep = e;
-        if (trunc && e) keep = wok && !(fabs(coef[c]) < thr);
-        mine += keep;
-      }
-#pragma unroll
-      for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(kFull, mine, o);
-      mine = __shfl_sync(kFull, mine, 0);
+    for (unsigned c = lane; c < size; c += 32) {
+      const bool e = (ex[c >> 5] >> (c & 31)) & 1u;
+      bool keep = e;
+      if (trunc && e) keep = wok && !(fabs(coef[c]) < thr);
+      mine += keep;
     }
-    if (lane == 0) s_cnt[warp] = active ? mine : 0u;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned run = 0;
-      for (int w = 0; w < kRunWarps; ++w) {
-        const unsigned t = s_cnt[w];
-        s_cnt[w] = run;
-        run += t;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(kFull, mine, o);
+    mine = __shfl_sync(kFull, mine, 0);
+    const unsigned long long excl = warp_lookback(ts, g, mine, epoch, ctrl, op);
+    unsigned long long out = ubase + excl;
+    for (unsigned c0 = 0; c0 < size; c0 += 32) {
+      const unsigned c = c0 + lane;
+      bool keep = false;
+      if (c < size) {
+        keep = (ex[c >> 5] >> (c & 31)) & 1u;
+        if (trunc && keep) keep = wok && !(fabs(coef[c]) < thr);
       }
-      s_cnt[kRunWarps] = run;
-    }
-    __syncthreads();
-    const unsigned agg = s_cnt[kRunWarps];
-    const unsigned long long excl = lookback(ts, tile, agg, epoch, ctrl, op, &s_slot);
-    if (active) {
-      unsigned long long out = ubase + excl + s_cnt[warp];
-      for (unsigned c0 = 0; c0 < size; c0 += 32) {
-        const unsigned c = c0 + lane;
-        bool keep = false;
-        if (c < size) {
-          keep = (ex[c >> 5] >> (c & 31)) & 1u;
-          if (trunc && keep) keep = wok && !(fabs(coef[c]) < thr);
-        }
-        const unsigned bal = __ballot_sync(kFull, keep);
-        if (keep) {
-          const unsigned long long r = out + __popc(bal & ((1u << lane) - 1u));
-          if (r < O.cap) {
-            uint64_t f[W], x[W], z[W];
+      const unsigned bal = __ballot_sync(kFull, keep);
+      if (keep) {
+        const unsigned long long r = out + __popc(bal & ((1u << lane) - 1u));
+        if (r < O.cap) {
+          uint64_t f[W], x[W], z[W];
 #pragma unroll
-            for (int w = 0; w < W; ++w) f[w] = f0[w];
-            for (unsigned t = 0; t < k; ++t)
-              if ((c >> t) & 1u) f[pos[t] >> 6] |= 1ull << (pos[t] & 63);
+          for (int w = 0; w < W; ++w) f[w] = f0[w];
+          for (unsigned t = 0; t < k; ++t)
+            if ((c >> t) & 1u) {
+              const unsigned q = pos[t];
 #pragma unroll
-            for (int w = 0; w < W; ++w) {
-              x[w] = cls == 0 ? f[w] : v[w];
-              z[w] = cls == 0 ? v[w] : f[w];
+              for (int w = 0; w < W; ++w)
+                if (w == (int)(q >> 6)) f[w] |= 1ull << (q & 63);
             }
-            store_key<W>(O, r, x, z);
-            O.c[r] = coef[c];
+#pragma unroll
+          for (int w = 0; w < W; ++w) {
+            x[w] = cls == 0 ? f[w] : v[w];
+            z[w] = cls == 0 ? v[w] : f[w];
           }
+          store_key<W>(O, r, x, z);
+          O.c[r] = coef[c];
         }
-        out += __popc(bal);
       }
+      out += __popc(bal);
     }
-    if (tile == ntiles - 1 && threadIdx.x == 0) {
-      ctrl->cap_needed = ubase + excl + agg;
-      if (ubase + excl + agg > O.cap) set_err(ctrl, kErrCapacity, op);
+    if (g == ngroups - 1 && lane == 0) {
+      ctrl->cap_needed = ubase + excl + mine;
+      if (ubase + excl + mine > O.cap) set_err(ctrl, kErrCapacity, op);
     }
-    __syncthreads();
+    __syncwarp();  // coef, ex and s_ord of this warp are rewritten by its next group
   }
   __syncthreads();
   for (unsigned j = threadIdx.x; j < L; j += blockDim.x)
