@@ -86,11 +86,15 @@ def lattice_bonds(L: int) -> list[tuple[int, int]]:
 
 
 def kicked_ising_2d(L: int = 12, layers: int = 20, theta_h=0.6, theta_zz: float = -math.pi / 2,
-                    thr: float = 1e-5, max_weight: int | None = 10, obs=(6, 6)) -> Workload:
+                    thr: float = 1e-5, max_weight: int | None = 10, obs=None) -> Workload:
     """2D kicked Ising: each forward layer applies RX(theta_h) on every qubit, then RZZ(theta_zz)
     on all bonds.  theta_h may be a per-layer list.  At theta_zz = -pi/2 the RZZ layer is
-    Clifford (``clifford_angles``)."""
+    Clifford (``clifford_angles``).  Observable: Z at site ``obs`` (default the centre,
+    (L//2, L//2), which is (6, 6) on the 12 x 12 lattice)."""
     n = L * L
+    obs = (L // 2, L // 2) if obs is None else tuple(obs)
+    if not (0 <= obs[0] < L and 0 <= obs[1] < L):
+        raise ValueError(f"observable site {obs} is outside the {L}x{L} lattice")
     bonds = lattice_bonds(L)
     th = list(theta_h) if isinstance(theta_h, (list, tuple)) else [theta_h] * layers
     ops = []
@@ -104,7 +108,7 @@ def kicked_ising_2d(L: int = 12, layers: int = 20, theta_h=0.6, theta_zz: float 
 
 
 def kicked_ising_random_h(L: int = 10, layers: int = 30, seed: int = 2, lo: float = 0.4, hi: float = 0.8,
-                          thr: float = 1e-7, max_weight: int | None = None, obs=(5, 5)) -> Workload:
+                          thr: float = 1e-7, max_weight: int | None = None, obs=None) -> Workload:
     """2D kicked Ising with a seeded transverse angle per layer, theta_h ~ U[lo, hi]
     (splitmix64), RZZ(-pi/2) on every bond; observable Z at ``obs``."""
     rng = SplitMix64(seed)

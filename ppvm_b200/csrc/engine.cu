@@ -292,6 +292,14 @@ void free_scratch(ppvm_sum* s) {
   s->tstate = nullptr;
 }
 
+// The fused-run group tables in their clean state (grp_min all ones, counts zero).
+ppvm_status clear_run_tables(ppvm_sum* s) {
+  CUDA_TRY(cudaMemsetAsync(s->R.grp_min, 0xFF, sizeof(uint32_t) * s->table_cap, s->stream));
+  CUDA_TRY(cudaMemsetAsync(s->R.grp_cnt, 0, sizeof(uint32_t) * s->table_cap, s->stream));
+  CUDA_TRY(cudaMemsetAsync(s->R.created, 0, sizeof(unsigned long long) * kRunMaxGates, s->stream));
+  return PPVM_OK;
+}
+
 // (Re)allocates term storage of capacity new_cap, keeping the first n_host terms.
 ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   if (new_cap >= 0xFFFFFFF0ull) return fail(PPVM_ECAPACITY, "term capacity limit (2^32) exceeded");
@@ -333,7 +341,7 @@ ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   CUDA_TRY(pool_malloc((void**)&s->R.g_fill, sizeof(uint32_t) * new_cap));
   CUDA_TRY(pool_malloc((void**)&s->R.members, sizeof(uint32_t) * new_cap));
   CUDA_TRY(pool_malloc((void**)&s->R.created, sizeof(unsigned long long) * kRunMaxGates));
-  return PPVM_OK;
+  return clear_run_tables(s);
 }
 
 ppvm_status ensure_log(ppvm_sum* s, size_t nops) {
@@ -704,9 +712,8 @@ struct K {
     const void* d_rd_v = nullptr;
     PPVM_TRY(stage_put(s, &rd, sizeof(RunDesc), &d_rd_v));
     const RunDesc* d_rd = static_cast<const RunDesc*>(d_rd_v);
-    CUDA_TRY(cudaMemsetAsync(s->R.grp_min, 0xFF, sizeof(uint32_t) * tsize, s->stream));
-    CUDA_TRY(cudaMemsetAsync(s->R.grp_cnt, 0, sizeof(uint32_t) * tsize, s->stream));
-    CUDA_TRY(cudaMemsetAsync(s->R.created, 0, sizeof(unsigned long long) * kRunMaxGates, s->stream));
+    // grp_min, grp_cnt and created are clean here: k_run_scatter and k_run_commit reset what a
+    // run used, grow() clears them on allocation and run_list() after a device error
     const int trunc = trunc_op >= 0 ? 1 : 0;
     {
       ProfScope ps(s, F_RUN_CLASSIFY, op0, L);
@@ -1025,6 +1032,7 @@ ppvm_status run_list(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, const std::v
       return PPVM_OK;
     }
     if (s->prof) prof_collect(s, test_words);
+    PPVM_TRY(clear_run_tables(s));  // a run stopped part-way leaves its slots set
     // fused runs at or after the failing op did not run: give their buffers back
     for (int op0 : s->swaps)
       if (op0 >= c.err_op) std::swap(s->planes, s->alt);

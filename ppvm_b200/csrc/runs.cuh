@@ -223,6 +223,9 @@ k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long lo
   }
 }
 
+// Also hands the group table back clean: grp_min and grp_cnt were last read by k_run_order,
+// so every member resets its slot (same values from every member), and the next run needs
+// no clearing pass.  After a device error the host clears both arrays instead.
 static __global__ void __launch_bounds__(256) k_run_scatter(Ctrl* ctrl, RunScratch R) {
   if (ld_volatile_int(&ctrl->err)) return;
   const unsigned long long N = ld_volatile(&ctrl->n);
@@ -233,6 +236,8 @@ static __global__ void __launch_bounds__(256) k_run_scatter(Ctrl* ctrl, RunScrat
     const uint32_t o = R.grp_ord[s];
     const uint32_t pos = R.g_start[o] + atomicAdd(&R.g_fill[o], 1u);
     R.members[pos] = (uint32_t)i;
+    R.grp_min[s] = kNone;
+    R.grp_cnt[s] = 0u;
   }
 }
 
@@ -519,6 +524,7 @@ static __global__ void __launch_bounds__(kRunMaxGates) k_run_commit(Ctrl* ctrl, 
     log[op0 + j].n_new = mine;
     log[op0 + j].n_out = n0 + incl;
     log[op0 + j].n_s = 0;
+    R.created[j] = 0;  // clean for the next run
   }
   __syncthreads();
   if (j == 0) {

@@ -42,3 +42,12 @@ def test_batched_ranges():
     assert len(wls) == 64
     assert all(16 <= w.n_qubits <= 128 and 5 <= w.meta["steps"] <= 30 for w in wls)
     assert all(0.5 <= w.meta["h"] <= 1.5 for w in wls)
+
+
+def test_kicked_ising_observable_is_on_the_lattice():
+    import pytest
+
+    assert C.kicked_ising_2d(L=4, layers=1).observable[0][0] == "".join("Z" if q == 10 else "I" for q in range(16))
+    assert C.kicked_ising_2d().observable[0][0].index("Z") == 6 * 12 + 6
+    with pytest.raises(ValueError):
+        C.kicked_ising_2d(L=4, layers=1, obs=(6, 6))
