@@ -66,6 +66,17 @@ __device__ __forceinline__ int ld_volatile_int(const int* p) {
   return *reinterpret_cast<const volatile int*>(p);
 }
 
+// Waits until the grids this one depends on in its stream have completed and their writes
+// are visible.  Kernels of the single-sum engine start with it, so the host may launch them
+// with programmatic stream serialization: the launch overlaps the previous kernel's run.
+// Without such a launch it returns at once.
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // Let the next kernel of the stream be launched now: it is scheduled only once every block
+  // of this grid has started, and its blocks wait in their own pdl_wait() for this grid.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void set_err(Ctrl* ctrl, int code, int op) {
   if (atomicCAS(&ctrl->err, 0, code) == 0) ctrl->err_op = op;
 }

@@ -16,6 +16,7 @@
 #include <unordered_map>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -388,6 +389,36 @@ void stage_reset(ppvm_sum* s) {
   s->stage_cur = 0;
 }
 
+// Kernel launch with programmatic stream serialization: the kernel may be launched while
+// the previous kernel of the stream finishes, and waits for it in pdl_wait() (every kernel
+// launched this way starts with it).  PPVM_PDL=0 in the environment turns it off.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("PPVM_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st, Args... args) {
+  if (!pdl_enabled()) {
+    kern<<<grid, block, smem, st>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 unsigned grid_for(unsigned long long work, unsigned long long per_block, int max_per_sm) {
   unsigned long long g = (work + per_block - 1) / per_block;
   const unsigned long long cap = (unsigned long long)g_sm_count * max_per_sm;
@@ -660,24 +691,24 @@ struct K {
     const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
     {
       ProfScope ps(s, F_SCAN, op, 1);
-      k_rot_scan<W, kScanBlock, ITEMS><<<grid_for(nub, TILE, 8), kScanBlock, 0, s->stream>>>(
+      launch(k_rot_scan<W, kScanBlock, ITEMS>, grid_for(nub, TILE, 8), kScanBlock, 0, s->stream,
           P, s->d_ctrl, g, xmask, zmask, s->s_idx, s->s_rec, s->partner, s->tstate,
           s->next_tile_epoch(), op, s->d_log);
     }
     {
       ProfScope ps(s, F_PAIR, op, 1);
-      k_rot_pair<W><<<grid_for(nub, kPairBlock, 8), kPairBlock, 0, s->stream>>>(
+      launch(k_rot_pair<W>, grid_for(nub, kPairBlock, 8), kPairBlock, 0, s->stream,
           s->d_ctrl, g, s->s_rec, s->partner, s->table, s->table_cap, s->next_table_epoch(), op);
     }
     {
       ProfScope ps(s, F_APPLY, op, 1);
-      k_rot_apply<W, kScanBlock, ITEMS><<<grid_for(nub, TILE, 8), kScanBlock, 0, s->stream>>>(
+      launch(k_rot_apply<W, kScanBlock, ITEMS>, grid_for(nub, TILE, 8), kScanBlock, 0, s->stream,
           P, s->d_ctrl, g, sn, cs, s->s_idx, s->s_rec, s->partner, s->tstate, s->next_tile_epoch(),
           op, s->d_log);
     }
     {
       ProfScope ps(s, F_COMMIT, op, 1);
-      k_commit_rot<<<1, 1, 0, s->stream>>>(s->d_ctrl, op, s->d_log);
+      launch(k_commit_rot, 1, 1, 0, s->stream, s->d_ctrl, op, s->d_log);
     }
     s->n_ub = std::min<unsigned long long>(s->cap, 2 * s->n_ub);
   }
@@ -685,21 +716,21 @@ struct K {
   static void clifford(ppvm_sum* s, const DevOp* ops_dev, int nops, int op0) {
     const Planes P = s->planes_view();
     ProfScope ps(s, F_CLIFF, op0, nops);
-    k_clifford<W, kCliffBlock><<<grid_for(std::max<unsigned long long>(s->n_ub, 1), kCliffBlock, 16),
-                                 kCliffBlock, 0, s->stream>>>(P, s->d_ctrl, ops_dev, nops, op0, s->d_log);
+    launch(k_clifford<W, kCliffBlock>, grid_for(std::max<unsigned long long>(s->n_ub, 1), kCliffBlock, 16),
+           kCliffBlock, 0, s->stream, P, s->d_ctrl, ops_dev, nops, op0, s->d_log);
   }
 
   static void truncate(ppvm_sum* s, int op) {
     const Planes P = s->planes_view();
     {
       ProfScope ps(s, F_TRUNC, op, 1);
-      k_truncate<W, kScanBlock, ITEMS><<<grid_for(std::max<unsigned long long>(s->n_ub, 1), TILE, 8),
-                                         kScanBlock, 0, s->stream>>>(
+      launch(k_truncate<W, kScanBlock, ITEMS>, grid_for(std::max<unsigned long long>(s->n_ub, 1), TILE, 8),
+             kScanBlock, 0, s->stream,
           P, s->d_ctrl, s->thr, s->maxw, s->d_pres_keys, s->d_pres_table, s->pres_mask, s->npres,
           s->side, s->tstate, s->next_tile_epoch(), op, s->d_log);
     }
     ProfScope ps2(s, F_COMMIT, op, 1);
-    k_commit_truncate<W><<<1, 256, 0, s->stream>>>(P, s->d_ctrl, s->side, op, s->d_log);
+    launch(k_commit_truncate<W>, 1, 256, 0, s->stream, P, s->d_ctrl, s->side, op, s->d_log);
   }
 
   // Fused run of single-qubit RX (cls 0) or RZ (cls 1) rotations, ops[op0..op0+L), optionally
@@ -717,32 +748,32 @@ struct K {
     const int trunc = trunc_op >= 0 ? 1 : 0;
     {
       ProfScope ps(s, F_RUN_CLASSIFY, op0, L);
-      k_run_classify<W><<<grid_for(nub, 256, 8), 256, 0, s->stream>>>(P, s->d_ctrl, d_rd, s->R, s->table,
+      launch(k_run_classify<W>, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, d_rd, s->R, s->table,
                                                                        tsize - 1, s->next_table_epoch(), op0);
     }
     {
       ProfScope ps(s, F_RUN_ORDER, op0, L);
       const unsigned ea = s->next_tile_epoch(), eb = s->next_tile_epoch();
-      k_run_order<kScanBlock, 2><<<grid_for(nub, kScanBlock * 2, 8), kScanBlock, 0, s->stream>>>(
+      launch(k_run_order<kScanBlock, 2>, grid_for(nub, kScanBlock * 2, 8), kScanBlock, 0, s->stream,
           s->d_ctrl, s->R, s->tstate, s->tstate2, ea, eb, op0);
     }
     {
       ProfScope ps(s, F_RUN_SCATTER, op0, L);
-      k_run_scatter<<<grid_for(nub, 256, 8), 256, 0, s->stream>>>(s->d_ctrl, s->R);
+      launch(k_run_scatter, grid_for(nub, 256, 8), 256, 0, s->stream, s->d_ctrl, s->R);
     }
     {
       ProfScope ps(s, F_RUN_UNTOUCHED, op0, L);
-      k_run_untouched<W, kScanBlock, ITEMS><<<grid_for(nub, TILE, 8), kScanBlock, 0, s->stream>>>(
+      launch(k_run_untouched<W, kScanBlock, ITEMS>, grid_for(nub, TILE, 8), kScanBlock, 0, s->stream,
           P, O, s->d_ctrl, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0);
     }
     {
       ProfScope ps(s, F_RUN_GROUPS, op0, L);
-      k_run_groups<W><<<grid_for(nub, kRunWarps, 8), kRunWarps * 32, 0, s->stream>>>(
+      launch(k_run_groups<W>, grid_for(nub, kRunWarps, 8), kRunWarps * 32, 0, s->stream,
           P, O, s->d_ctrl, d_rd, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0);
     }
     {
       ProfScope ps(s, F_RUN_COMMIT, op0, L);
-      k_run_commit<<<1, kRunMaxGates, 0, s->stream>>>(s->d_ctrl, s->R, op0, L, trunc_op, s->d_log);
+      launch(k_run_commit, 1, kRunMaxGates, 0, s->stream, s->d_ctrl, s->R, op0, L, trunc_op, s->d_log);
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);
@@ -771,14 +802,13 @@ struct K {
     const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
     {
       ProfScope ps(s, F_TABLEAU, op0, nops, trunc_op);
-      k_tableau<W, kTabBlock, ITEMS><<<grid_for(nub, (unsigned long long)kTabBlock * ITEMS, bps), kTabBlock, smem,
-                                      s->stream>>>(
+      launch(k_tableau<W, kTabBlock, ITEMS>, grid_for(nub, (unsigned long long)kTabBlock * ITEMS, bps), kTabBlock, smem, s->stream,
           P, O, s->d_ctrl, t.tp, static_cast<const uint64_t*>(d_rows), static_cast<const uint8_t*>(d_ph),
           trunc_op >= 0 ? 1 : 0, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0, nops, s->d_log);
     }
     {
       ProfScope ps(s, F_COMMIT, op0, nops);
-      k_commit_tableau<<<1, 1, 0, s->stream>>>(s->d_ctrl, trunc_op, s->d_log);
+      launch(k_commit_tableau, 1, 1, 0, s->stream, s->d_ctrl, trunc_op, s->d_log);
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);

@@ -63,6 +63,7 @@ template <int W, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_rot_scan(Planes P, Ctrl* ctrl, Gen g, unsigned xmask, unsigned zmask, uint32_t* s_idx, uint64_t* s_rec,
            uint32_t* partner, unsigned long long* ts, unsigned epoch, int op, OpLog* log) {
+  pdl_wait();
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
   __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
@@ -132,6 +133,7 @@ template <int W>
 __global__ void __launch_bounds__(256)
 k_rot_pair(Ctrl* ctrl, Gen g, const uint64_t* s_rec, uint32_t* partner,
            unsigned long long* table, unsigned long long table_cap, unsigned tepoch, int op) {
+  pdl_wait();
   if (ld_volatile_int(&ctrl->err)) return;
   const unsigned long long ns = ld_volatile(&ctrl->n_s);
   if (ns == 0) return;
@@ -201,6 +203,7 @@ __global__ void __launch_bounds__(BLOCK)
 k_rot_apply(Planes P, Ctrl* ctrl, Gen g, double sn, double cs, const uint32_t* s_idx,
             const uint64_t* s_rec, const uint32_t* partner, unsigned long long* ts,
             unsigned epoch, int op, OpLog* log) {
+  pdl_wait();
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
   __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
@@ -276,6 +279,7 @@ k_rot_apply(Planes P, Ctrl* ctrl, Gen g, double sn, double cs, const uint32_t* s
 
 // Publishes the live count after a rotation and resets the tile tickets (one thread).
 static __global__ void k_commit_rot(Ctrl* ctrl, int op, OpLog* log) {
+  pdl_wait();
   for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
   if (ctrl->err) return;
   const unsigned long long nchild = ctrl->n_s - 2 * ctrl->n_pairs;
@@ -313,6 +317,7 @@ __global__ void __launch_bounds__(BLOCK)
 k_truncate(Planes P, Ctrl* ctrl, double thr, unsigned long long maxw, const uint64_t* pres_keys,
            const int* pres_table, unsigned pres_mask, int npres, uint64_t* side,
            unsigned long long* ts, unsigned epoch, int op, OpLog* log) {
+  pdl_wait();
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
   __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
@@ -386,6 +391,7 @@ k_truncate(Planes P, Ctrl* ctrl, double thr, unsigned long long maxw, const uint
 // Appends the preserved-but-dropped terms after the kept ones and publishes the count.
 template <int W>
 __global__ void k_commit_truncate(Planes P, Ctrl* ctrl, const uint64_t* side, int op, OpLog* log) {
+  pdl_wait();
   if (threadIdx.x == 0 && blockIdx.x == 0)
     for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
   if (ld_volatile_int(&ctrl->err)) return;
@@ -429,6 +435,7 @@ constexpr int kCliffBlock = 128;
 template <int W, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_clifford(Planes P, Ctrl* ctrl, const DevOp* ops, int nops, int op0, OpLog* log) {
+  pdl_wait();
   __shared__ DevOp s_ops[kMaxOpsPerLaunch];
   __shared__ uint64_t s_x[W][BLOCK];
   __shared__ uint64_t s_z[W][BLOCK];
@@ -579,6 +586,7 @@ __device__ __forceinline__ double block_sum(double v, double* s_red) {
 // Sum of coefficients of words without X bits: trace("Z?*") = overlap_with_zero.
 template <int W>
 __global__ void __launch_bounds__(256) k_owz(Planes P, const Ctrl* ctrl, double* partials) {
+  pdl_wait();
   __shared__ double s_red[8];
   const unsigned long long N = ld_volatile(&ctrl->n);
   double acc = 0.0;
@@ -594,6 +602,7 @@ __global__ void __launch_bounds__(256) k_owz(Planes P, const Ctrl* ctrl, double*
 }
 
 static __global__ void k_sum_partials(const double* partials, int n, Ctrl* ctrl) {
+  pdl_wait();
   __shared__ double s_red[8];
   double acc = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) acc = __dadd_rn(acc, partials[i]);

@@ -67,6 +67,7 @@ template <int W>
 __global__ void __launch_bounds__(256)
 k_run_classify(Planes P, Ctrl* ctrl, const RunDesc* rd, RunScratch R, unsigned long long* table,
                unsigned long long tmask, unsigned tepoch, int op) {
+  pdl_wait();
   if (ld_volatile_int(&ctrl->err)) return;
   const unsigned long long N = ld_volatile(&ctrl->n);
   const uint32_t cls = rd->cls;
@@ -132,6 +133,7 @@ template <int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long long* ts_b, unsigned ep_a,
             unsigned ep_b, int op) {
+  pdl_wait();
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
   __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
@@ -227,6 +229,7 @@ k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long lo
 // so every member resets its slot (same values from every member), and the next run needs
 // no clearing pass.  After a device error the host clears both arrays instead.
 static __global__ void __launch_bounds__(256) k_run_scatter(Ctrl* ctrl, RunScratch R) {
+  pdl_wait();
   if (ld_volatile_int(&ctrl->err)) return;
   const unsigned long long N = ld_volatile(&ctrl->n);
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
@@ -247,6 +250,7 @@ template <int W, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_run_untouched(Planes P, Planes O, Ctrl* ctrl, RunScratch R, int trunc, double thr, unsigned long long maxw,
                 unsigned long long* ts, unsigned epoch, int op) {
+  pdl_wait();
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
   __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
@@ -303,6 +307,7 @@ template <int W>
 __global__ void __launch_bounds__(kRunWarps * 32)
 k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, int trunc, double thr,
              unsigned long long maxw, unsigned long long* ts, unsigned epoch, int op) {
+  pdl_wait();
   constexpr int SZ = 1 << kRunMaxK;
   __shared__ double s_coef[kRunWarps][SZ];
   __shared__ unsigned s_ex[kRunWarps][SZ / 32];
@@ -495,6 +500,7 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
 // counts gives each gate's live count).
 static __global__ void __launch_bounds__(kRunMaxGates) k_run_commit(Ctrl* ctrl, RunScratch R, int op0, int L,
                                                                     int trunc_op, OpLog* log) {
+  pdl_wait();
   __shared__ unsigned long long s_w[kRunMaxGates / 32];
   __shared__ int s_err;
   if (threadIdx.x == 0) s_err = ctrl->err;

@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(BLOCK)
 k_tableau(Planes P, Planes O, Ctrl* ctrl, TabParams tp, const uint64_t* __restrict__ g_rows,
           const uint8_t* __restrict__ g_ph, int trunc, double thr, unsigned long long maxw,
           unsigned long long* ts, unsigned epoch, int op0, int nops, OpLog* log) {
+  pdl_wait();
   extern __shared__ __align__(16) uint64_t s_rows[];  // nrows * 2W words, then nrows phase bytes
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
@@ -215,6 +216,7 @@ k_tableau(Planes P, Planes O, Ctrl* ctrl, TabParams tp, const uint64_t* __restri
 
 // Publishes the count after a tableau pass (and fills the log of its fused TRUNCATE).
 static __global__ void k_commit_tableau(Ctrl* ctrl, int trunc_op, OpLog* log) {
+  pdl_wait();
   for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
   if (ctrl->err) return;
   const unsigned long long n_in = ctrl->n, n_out = ctrl->n_s;
