@@ -473,8 +473,7 @@ uint64_t launch_bytes(const ppvm_sum* s, const ProfLaunch& L, const std::vector<
     case F_APPLY: return g.n_s * (B + 8) + g.n_new * B;  // records, coeff writes, children
     case F_CLIFF: return 2ull * g.n_in * B;
     case F_TRUNC: return g.n_in * B + g.n_out * B;
-    case F_RUN_CLASSIFY: return g.n_in * B;                    // every term's key read once
-    case F_RUN_UNTOUCHED: return g.n_in * 8 + g.n_in * B;      // group slots + untouched terms
+    case F_RUN_CLASSIFY: return g.n_in * B + g.n_in * 4;       // every term read once, group slots
     case F_TABLEAU: {  // every term read once, survivors written once
       const uint64_t out = L.aux >= 0 ? s->h_log[L.aux].n_out : g.n_in;
       return g.n_in * B + out * B;
@@ -748,8 +747,10 @@ struct K {
     const int trunc = trunc_op >= 0 ? 1 : 0;
     {
       ProfScope ps(s, F_RUN_CLASSIFY, op0, L);
-      launch(k_run_classify<W>, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, d_rd, s->R, s->table,
-                                                                       tsize - 1, s->next_table_epoch(), op0);
+      const unsigned tep = s->next_table_epoch();
+      launch(k_run_classify<W, kScanBlock, ITEMS>, grid_for(nub, TILE, 8), kScanBlock, 0, s->stream, P, O,
+             s->d_ctrl, d_rd, s->R, s->table, tsize - 1, tep, trunc, s->thr, s->maxw, s->tstate,
+             s->next_tile_epoch(), op0);
     }
     {
       ProfScope ps(s, F_RUN_ORDER, op0, L);
@@ -760,11 +761,6 @@ struct K {
     {
       ProfScope ps(s, F_RUN_SCATTER, op0, L);
       launch(k_run_scatter, grid_for(nub, 256, 8), 256, 0, s->stream, s->d_ctrl, s->R);
-    }
-    {
-      ProfScope ps(s, F_RUN_UNTOUCHED, op0, L);
-      launch(k_run_untouched<W, kScanBlock, ITEMS>, grid_for(nub, TILE, 8), kScanBlock, 0, s->stream,
-          P, O, s->d_ctrl, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0);
     }
     {
       ProfScope ps(s, F_RUN_GROUPS, op0, L);

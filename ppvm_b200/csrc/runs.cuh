@@ -15,10 +15,10 @@
 // and every coefficient are identical to the reference's; only the output order differs
 // (untouched terms in order, then groups by their first member, members by coordinate).
 //
-// Kernels, in order: k_run_classify (group keys into a hash table, members counted),
-// k_run_order (deterministic group numbering by first member, member offsets),
-// k_run_scatter (member lists), k_run_untouched (terms outside every group, compacted),
-// k_run_groups (butterfly + truncation + ordered write), k_run_commit (counts, op log).
+// Kernels, in order: k_run_classify (group keys into a hash table, members counted; terms
+// outside every group compacted to the output with the truncation), k_run_order
+// (deterministic group numbering by first member, member offsets), k_run_scatter (member
+// lists), k_run_groups (butterfly + truncation + ordered write), k_run_commit (counts, op log).
 #pragma once
 
 #include "kernels.cuh"
@@ -63,68 +63,112 @@ __device__ __forceinline__ void split_planes(uint32_t cls, const uint64_t (&x)[W
 }
 
 // ---------------------------------------------------------------------------------------
-template <int W>
-__global__ void __launch_bounds__(256)
-k_run_classify(Planes P, Ctrl* ctrl, const RunDesc* rd, RunScratch R, unsigned long long* table,
-               unsigned long long tmask, unsigned tepoch, int op) {
+// Classifies every term and, in the same pass, writes the terms the run does not touch
+// (no qubit of the run in the invariant plane) to the front of the output planes, in index
+// order, with the run's TRUNCATE applied to them (tile ranks + decoupled look-back).  Touched
+// terms join their group in the hash table.
+template <int W, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK)
+k_run_classify(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, unsigned long long* table,
+               unsigned long long tmask, unsigned tepoch, int trunc, double thr, unsigned long long maxw,
+               unsigned long long* ts, unsigned epoch, int op) {
   pdl_wait();
-  if (ld_volatile_int(&ctrl->err)) return;
+  __shared__ unsigned s_tile;
+  __shared__ unsigned long long s_slot;
+  __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
+  __shared__ int s_err;
+  if (threadIdx.x == 0) s_err = ld_volatile_int(&ctrl->err);
+  __syncthreads();
+  if (s_err) return;
   const unsigned long long N = ld_volatile(&ctrl->n);
+  constexpr unsigned long long TILE = (unsigned long long)BLOCK * ITEMS;
+  const unsigned long long ntiles = (N + TILE - 1) / TILE;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && N == 0) ctrl->n_s = 0;
   const uint32_t cls = rd->cls;
   uint64_t Q[W];
 #pragma unroll
   for (int w = 0; w < W; ++w) Q[w] = rd->Q[w];
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
-       i += (unsigned long long)gridDim.x * blockDim.x) {
-    uint64_t x[W], z[W], v[W], f[W], M[W];
-    load_key<W>(P, i, x, z);
-    split_planes<W>(cls, x, z, v, f);
-    unsigned k = 0;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = BLOCK / 32;
+  const bool wcap = maxw != ~0ull;
+  for (;;) {
+    const unsigned tile = next_tile(&ctrl->tickets[1], &s_tile);
+    if (tile >= ntiles) break;
+    const unsigned long long base = (unsigned long long)tile * TILE;
+    uint64_t kx[ITEMS][W], kz[ITEMS][W];
+    double kc[ITEMS];
+    unsigned bal[ITEMS];
 #pragma unroll
-    for (int w = 0; w < W; ++w) {
-      M[w] = v[w] & Q[w];
-      k += __popcll(M[w]);
-      f[w] &= ~M[w];
-    }
-    if (k == 0) {
-      R.gslot[i] = kNone;
-      continue;
-    }
-    if (k > (unsigned)kRunMaxK) {
-      set_err(ctrl, kErrFallback, op);
-      R.gslot[i] = kNone;
-      continue;
-    }
-    const uint64_t h = hash_key<W>(v, f);
-    const unsigned tag = (unsigned)(h >> 48) & 0xFFFFu;
-    const unsigned long long mine = make_slot(tepoch, tag, (unsigned)i);
-    unsigned long long slot = h & tmask;
-    unsigned long long probes = 0;
-    while (true) {
-      const unsigned long long cur = ld_volatile(&table[slot]);
-      if (slot_epoch(cur) != (tepoch & 0xFFFFu)) {
-        const unsigned long long prev = atomicCAS(&table[slot], cur, mine);
-        if (prev != cur) continue;
-        break;  // new group
-      }
-      if (slot_tag(cur) == tag) {
-        uint64_t jx[W], jz[W], jv[W], jf[W];
-        load_key<W>(P, slot_idx(cur), jx, jz);
-        split_planes<W>(cls, jx, jz, jv, jf);
-        bool eq = true;
+    for (int it = 0; it < ITEMS; ++it) {
+      const unsigned long long i = base + (unsigned long long)it * BLOCK + threadIdx.x;
+      bool keep = false;
+      if (i < N) {
+        uint64_t v[W], f[W], M[W];
+        load_key<W>(P, i, kx[it], kz[it]);
+        split_planes<W>(cls, kx[it], kz[it], v, f);
+        unsigned k = 0;
 #pragma unroll
-        for (int w = 0; w < W; ++w) eq &= (jv[w] == v[w]) & ((jf[w] & ~M[w]) == f[w]);
-        if (eq) break;  // same group
+        for (int w = 0; w < W; ++w) {
+          M[w] = v[w] & Q[w];
+          k += __popcll(M[w]);
+          f[w] &= ~M[w];
+        }
+        if (k == 0) {  // untouched by the run
+          R.gslot[i] = kNone;
+          kc[it] = P.c[i];
+          keep = true;
+          if (trunc) {
+            keep = !(fabs(kc[it]) < thr);
+            if (wcap) keep = keep && (weight<W>(kx[it], kz[it]) <= maxw);
+          }
+        } else if (k > (unsigned)kRunMaxK) {
+          set_err(ctrl, kErrFallback, op);
+          R.gslot[i] = kNone;
+        } else {
+          const uint64_t h = hash_key<W>(v, f);
+          const unsigned tag = (unsigned)(h >> 48) & 0xFFFFu;
+          const unsigned long long mine = make_slot(tepoch, tag, (unsigned)i);
+          unsigned long long slot = h & tmask;
+          unsigned long long probes = 0;
+          while (true) {
+            const unsigned long long cur = ld_volatile(&table[slot]);
+            if (slot_epoch(cur) != (tepoch & 0xFFFFu)) {
+              const unsigned long long prev = atomicCAS(&table[slot], cur, mine);
+              if (prev != cur) continue;
+              break;  // new group
+            }
+            if (slot_tag(cur) == tag) {
+              uint64_t jx[W], jz[W], jv[W], jf[W];
+              load_key<W>(P, slot_idx(cur), jx, jz);
+              split_planes<W>(cls, jx, jz, jv, jf);
+              bool eq = true;
+#pragma unroll
+              for (int w = 0; w < W; ++w) eq &= (jv[w] == v[w]) & ((jf[w] & ~M[w]) == f[w]);
+              if (eq) break;  // same group
+            }
+            slot = (slot + 1) & tmask;
+            if (++probes > tmask) {
+              set_err(ctrl, kErrProbe, op);
+              break;
+            }
+          }
+          R.gslot[i] = (uint32_t)slot;
+          atomicMin(&R.grp_min[slot], (uint32_t)i);
+          atomicAdd(&R.grp_cnt[slot], 1u);
+        }
       }
-      slot = (slot + 1) & tmask;
-      if (++probes > tmask) {
-        set_err(ctrl, kErrProbe, op);
-        break;
-      }
+      bal[it] = __ballot_sync(kFull, keep);
     }
-    R.gslot[i] = (uint32_t)slot;
-    atomicMin(&R.grp_min[slot], (uint32_t)i);
-    atomicAdd(&R.grp_cnt[slot], 1u);
+    const unsigned agg = tile_ranks<BLOCK, ITEMS>(bal, s_base);
+    const unsigned long long excl = lookback(ts, tile, agg, epoch, ctrl, op, &s_slot);
+#pragma unroll
+    for (int it = 0; it < ITEMS; ++it)
+      if ((bal[it] >> lane) & 1u) {
+        const unsigned long long r = excl + s_base[it * NW + warp] + __popc(bal[it] & ((1u << lane) - 1u));
+        store_key<W>(O, r, kx[it], kz[it]);
+        O.c[r] = kc[it];
+      }
+    if (tile == ntiles - 1 && threadIdx.x == 0) ctrl->n_s = excl + agg;
   }
 }
 
@@ -241,61 +285,6 @@ static __global__ void __launch_bounds__(256) k_run_scatter(Ctrl* ctrl, RunScrat
     R.members[pos] = (uint32_t)i;
     R.grp_min[s] = kNone;
     R.grp_cnt[s] = 0u;
-  }
-}
-
-// Terms outside every group: unchanged by the run; compacted (with the truncation that ends
-// the run, if any) to the front of the output planes, in index order.
-template <int W, int BLOCK, int ITEMS>
-__global__ void __launch_bounds__(BLOCK)
-k_run_untouched(Planes P, Planes O, Ctrl* ctrl, RunScratch R, int trunc, double thr, unsigned long long maxw,
-                unsigned long long* ts, unsigned epoch, int op) {
-  pdl_wait();
-  __shared__ unsigned s_tile;
-  __shared__ unsigned long long s_slot;
-  __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
-  if (ld_volatile_int(&ctrl->err)) return;
-  const unsigned long long N = ld_volatile(&ctrl->n);
-  constexpr unsigned long long TILE = (unsigned long long)BLOCK * ITEMS;
-  const unsigned long long ntiles = (N + TILE - 1) / TILE;
-  if (blockIdx.x == 0 && threadIdx.x == 0 && N == 0) ctrl->n_s = 0;
-  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int NW = BLOCK / 32;
-  const bool wcap = maxw != ~0ull;
-  for (;;) {
-    const unsigned tile = next_tile(&ctrl->tickets[1], &s_tile);
-    if (tile >= ntiles) break;
-    const unsigned long long base = (unsigned long long)tile * TILE;
-    unsigned ballots[ITEMS];
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
-      bool keep = false;
-      if (i < N && R.gslot[i] == kNone) {
-        keep = true;
-        if (trunc) {
-          uint64_t x[W], z[W];
-          load_key<W>(P, i, x, z);
-          keep = !(fabs(P.c[i]) < thr);
-          if (wcap) keep = keep && (weight<W>(x, z) <= maxw);
-        }
-      }
-      ballots[k] = __ballot_sync(kFull, keep);
-    }
-    const unsigned agg = tile_ranks<BLOCK, ITEMS>(ballots, s_base);
-    const unsigned long long excl = lookback(ts, tile, agg, epoch, ctrl, op, &s_slot);
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      if ((ballots[k] >> lane) & 1u) {
-        const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
-        const unsigned long long r = excl + s_base[k * NW + warp] + __popc(ballots[k] & ((1u << lane) - 1u));
-        uint64_t x[W], z[W];
-        load_key<W>(P, i, x, z);
-        store_key<W>(O, r, x, z);
-        O.c[r] = P.c[i];
-      }
-    }
-    if (tile == ntiles - 1 && threadIdx.x == 0) ctrl->n_s = excl + agg;
   }
 }
 
