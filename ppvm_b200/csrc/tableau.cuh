@@ -108,6 +108,48 @@ struct TabParams {
   uint32_t nrows;       // 2 * touched: row 2r = image of X_q, 2r+1 = image of Z_q (r = rank of q)
 };
 
+// Maps the word (x, z) through the composed run: (ox, oz) receives the image word, and the
+// return value e is the sign's phase, image = i^e * (Hermitian word): e = 0 or 2 (sign -1);
+// an odd e would mean a broken table.  rows/ph: the image table (shared or global memory).
+template <int W>
+__device__ __forceinline__ unsigned tab_map(const uint64_t* rows, const uint8_t* ph, const TabParams& tp,
+                                            const uint64_t (&x)[W], const uint64_t (&z)[W], uint64_t (&ox)[W],
+                                            uint64_t (&oz)[W]) {
+  unsigned p = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    p += __popcll(x[w] & z[w]);
+    ox[w] = x[w] & ~tp.T[w];
+    oz[w] = z[w] & ~tp.T[w];
+  }
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      uint64_t m = (s == 0 ? x[w] : z[w]) & tp.T[w];
+      while (m) {
+        const int b = __ffsll((long long)m) - 1;
+        m &= m - 1;
+        const unsigned row = 2u * (tp.pre[w] + __popcll(tp.T[w] & ((1ull << b) - 1ull))) + s;
+        const uint64_t* e = rows + (size_t)row * 2 * W;
+        unsigned t = 0;
+#pragma unroll
+        for (int ww = 0; ww < W; ++ww) {
+          const uint64_t a = e[ww];
+          t += __popcll(oz[ww] & a);
+          ox[ww] ^= a;
+          oz[ww] ^= e[W + ww];
+        }
+        p += ph[row] + 2u * t;
+      }
+    }
+  }
+  unsigned hw = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) hw += __popcll(ox[w] & oz[w]);
+  return (p - hw) & 3u;
+}
+
 // Maps every live term through the run; with trunc, drops what the strategy drops.  Survivors
 // go to O in input order; the count is left in ctrl->n_s for k_commit_tableau.
 template <int W, int BLOCK, int ITEMS>
@@ -157,39 +199,7 @@ k_tableau(Planes P, Planes O, Ctrl* ctrl, TabParams tp, const uint64_t* __restri
         uint64_t x[W], z[W];
         load_key<W>(P, i, x, z);
         const double c = P.c[i];
-        unsigned p = 0;
-#pragma unroll
-        for (int w = 0; w < W; ++w) {
-          p += __popcll(x[w] & z[w]);
-          ox[k][w] = x[w] & ~tp.T[w];
-          oz[k][w] = z[w] & ~tp.T[w];
-        }
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-#pragma unroll
-          for (int w = 0; w < W; ++w) {
-            uint64_t m = (s == 0 ? x[w] : z[w]) & tp.T[w];
-            while (m) {
-              const int b = __ffsll((long long)m) - 1;
-              m &= m - 1;
-              const unsigned row = 2u * (tp.pre[w] + __popcll(tp.T[w] & ((1ull << b) - 1ull))) + s;
-              const uint64_t* e = s_rows + (size_t)row * 2 * W;
-              unsigned t = 0;
-#pragma unroll
-              for (int ww = 0; ww < W; ++ww) {
-                const uint64_t a = e[ww];
-                t += __popcll(oz[k][ww] & a);
-                ox[k][ww] ^= a;
-                oz[k][ww] ^= e[W + ww];
-              }
-              p += s_ph[row] + 2u * t;
-            }
-          }
-        }
-        unsigned hw = 0;
-#pragma unroll
-        for (int w = 0; w < W; ++w) hw += __popcll(ox[k][w] & oz[k][w]);
-        const unsigned e = (p - hw) & 3u;
+        const unsigned e = tab_map<W>(s_rows, s_ph, tp, x, z, ox[k], oz[k]);
         if (e & 1u) set_err(ctrl, kErrProbe, op0);  // not a Hermitian image: internal error
         oc[k] = (e == 2u) ? -c : c;
         keep = true;

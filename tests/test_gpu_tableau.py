@@ -10,6 +10,7 @@ import random
 import numpy as np
 import pytest
 
+from ppvm_b200 import circuits as C
 from ppvm_b200 import gates as G
 from ppvm_b200.paulisum import PauliSum
 from tests.helpers import oracle_from, planes
@@ -83,3 +84,35 @@ def test_tableau_live_counts_and_log():
     want = o.run_ops(ops, counts=True)
     assert np.array_equal(g.live_counts(), want)
     same(g, o)
+
+
+@pytest.mark.parametrize("trunc_between", [True, False])
+def test_clifford_segment_folded_into_the_next_rx_run(trunc_between):
+    # a Clifford segment (>= 8 ops) right before a fused RX run is applied inside the run's
+    # passes; the replays after a group too large for the run (2^12 coordinates) and after a
+    # capacity overflow must restart at the segment
+    n = 12
+    segment = [G.g1(G.H, q) for q in range(n)] + [G.g2(G.CNOT, q, q + 1) for q in range(n - 1)]
+    rx = [G.r1(G.RX, q, 0.3 + 0.01 * q) for q in range(n)]
+    ops = segment + ([G.truncate()] if trunc_between else []) + rx + [G.truncate()]
+    for terms in ([("X" * n, 1.0)], [("XIXIXIXIXIXI", 0.5), ("ZZIIYYIIXXII", -0.25)]):
+        for cap in (0, 1):
+            g = gpu_from(terms, n, thr=1e-9, maxw=None, clifford_angles=True, capacity=cap, exact=False)
+            o = oracle_from(terms, n, thr=1e-9, clifford_angles=True)
+            g.run(ops)
+            want = o.run_ops(ops, counts=True)
+            from tests.test_gpu_parity import same_set
+            same_set(g, o)
+            assert np.array_equal(g.live_counts(), want)
+            assert abs(g.overlap_with_zero() - o.overlap_with_zero()) < 1e-10
+
+
+def test_folded_segment_with_weight_cap_keeps_counts():
+    wl = C.kicked_ising_2d(L=6, layers=5, thr=1e-5, max_weight=6)
+    g = gpu_from(wl.observable, wl.n_qubits, wl.min_abs_coeff, wl.max_weight, True, exact=False)
+    o = oracle_from(wl.observable, wl.n_qubits, wl.min_abs_coeff, wl.max_weight, True)
+    g.run(wl.ops)
+    want = o.run_ops(wl.ops, counts=True)
+    from tests.test_gpu_parity import same_set
+    same_set(g, o)
+    assert np.array_equal(g.live_counts(), want)
