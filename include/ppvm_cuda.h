@@ -55,6 +55,7 @@ typedef enum ppvm_opcode {
   PPVM_OP_DEPOLARIZE1,                                   /* q0, theta = p */
   PPVM_OP_DEPOLARIZE2,                                   /* q0, q1, theta = p */
   PPVM_OP_TRUNCATE,                                      /* run the strategy */
+  PPVM_OP_AMPLITUDE_DAMPING,                             /* q0, theta = gamma */
   PPVM_OP_COUNT_
 } ppvm_opcode;
 
@@ -157,6 +158,17 @@ ppvm_status ppvm_pauli_error(ppvm_sum* sum, const uint32_t* targets, size_t k, c
 ppvm_status ppvm_depolarize1(ppvm_sum* sum, const uint32_t* targets, size_t k, double p, int truncate);
 ppvm_status ppvm_depolarize2(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, double p,
                              int truncate);
+/* TwoQubitPauliError::two_qubit_pauli_error (noise.rs:39-105), applied pair by pair
+ * (two_qubit_pauli_error_many, crates/ppvm-traits/src/traits/noise.rs:77-81).  p[0..15) are
+ * the probabilities of IX IY IZ XI XX XY XZ YI YX YY YZ ZI ZX ZY ZZ, first letter on the
+ * pair's first qubit; a term is scaled by 1 - 2 * (sum of the p of the Paulis that
+ * anticommute with it on the pair).  Odd k_flat: PPVM_EINVAL. */
+ppvm_status ppvm_two_qubit_pauli_error(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat,
+                                       const double p[15], int truncate);
+/* AmplitudeDamping::amplitude_damping (noise.rs:132-163) on qubit q, Heisenberg adjoint:
+ * Z -> (1 - gamma) Z + gamma I, X/Y -> sqrt(1 - gamma) X/Y, I -> I.  The I child merges
+ * into an existing term with `+=` or is appended in parent order, as map_insert does. */
+ppvm_status ppvm_amplitude_damping(ppvm_sum* sum, uint32_t q, double gamma, int truncate);
 
 /* ---- truncation, readout ---------------------------------------------------------- */
 /* PauliSum::truncate (data.rs:275-311) with CombinedStrategy(CoefficientThreshold, MaxPauliWeight)

@@ -386,6 +386,52 @@ struct OSum {
     });
   }
 
+  // two_qubit_pauli_error (noise.rs:39-105).  A term with Paulis (Pa, Pb) on the pair is
+  // scaled by acc = 1 - 2 p[i1] - 2 p[i2] - ... - 2 p[i8] over the eight two-qubit Paulis that
+  // anticommute with it, subtracted in the reference's index order (the order fixes the
+  // rounding).  Rows by (code a, code b), code = x | z << 1 (I 0, X 1, Z 2, Y 3); p indices
+  // name IX IY IZ XI XX XY XZ YI YX YY YZ ZI ZX ZY ZZ in that order.
+  void two_qubit_pauli_error(uint32_t a, uint32_t b, const double p[15]) {
+    static const int8_t kIdx[4][4][8] = {
+        {{-1}, {1, 10, 13, 14, 2, 5, 6, 9}, {0, 1, 12, 13, 4, 5, 8, 9}, {0, 10, 12, 14, 2, 4, 6, 8}},
+        {{10, 11, 12, 13, 14, 7, 8, 9}, {1, 11, 12, 2, 5, 6, 7, 8}, {0, 1, 10, 11, 14, 4, 5, 7},
+         {0, 11, 13, 2, 4, 6, 7, 9}},
+        {{10, 3, 4, 5, 6, 7, 8, 9}, {1, 13, 14, 2, 3, 4, 7, 8}, {0, 1, 10, 12, 13, 3, 6, 7},
+         {0, 12, 14, 2, 3, 5, 7, 9}},
+        {{11, 12, 13, 14, 3, 4, 5, 6}, {1, 10, 11, 12, 2, 3, 4, 9}, {0, 1, 11, 14, 3, 6, 8, 9},
+         {0, 10, 11, 13, 2, 3, 5, 8}}};
+    double f[4][4];
+    for (int ca = 0; ca < 4; ++ca)
+      for (int cb = 0; cb < 4; ++cb) {
+        double acc = 1.0;
+        if (ca | cb)
+          for (int t = 0; t < 8; ++t) acc = acc - p[kIdx[ca][cb][t]] * 2.0;
+        f[ca][cb] = acc;
+      }
+    scale([&](const uint64_t* k, double& v) {
+      const int ca = (int)get_x(k, a) | ((int)get_z(k, a) << 1);
+      const int cb = (int)get_x(k, b) | ((int)get_z(k, b) << 1);
+      if (ca | cb) v *= f[ca][cb];
+    });
+  }
+  // amplitude_damping (noise.rs:132-163): I unchanged; X, Y scaled by sqrt(1 - gamma); Z
+  // scaled by (1 - gamma) with the child (Z -> I on q, v * gamma) collected by map_insert.
+  void amplitude_damping(uint32_t q, double gamma) {
+    const double om = 1.0 - gamma;
+    const double sxy = std::sqrt(om);
+    map_insert([&](uint64_t* ck, double& v, double& cv) {
+      if (get_x(ck, q)) {
+        v *= sxy;
+        return false;
+      }
+      if (!get_z(ck, q)) return false;
+      cv = v * gamma;
+      set_z(ck, q, false);
+      v *= om;
+      return true;
+    });
+  }
+
   // ---- truncation (data.rs:275-311, strategy.rs) -------------------------------------
   void strategy() {
     double t = thr;
@@ -575,6 +621,7 @@ int run_op(OSum* s, const ppvm_op& op) {
     case PPVM_OP_DEPOLARIZE1: if (!qok(s, op.q0)) return 1; s->depolarize1(op.q0, op.theta); return 0;
     case PPVM_OP_DEPOLARIZE2: if (!two_ok()) return 1; s->depolarize2(op.q0, op.q1, op.theta); return 0;
     case PPVM_OP_TRUNCATE: s->truncate(); return 0;
+    case PPVM_OP_AMPLITUDE_DAMPING: if (!qok(s, op.q0)) return 1; s->amplitude_damping(op.q0, op.theta); return 0;
     default: return 1;
   }
 }
@@ -607,6 +654,17 @@ int oracle_add_terms(void* h, const uint64_t* x, const uint64_t* z, const double
     for (int w = 0; w < s->W; ++w) { key[w] = x[i * s->W + w]; key[s->W + w] = z[i * s->W + w]; }
     s->add_assign(key.data(), c[i]);
   }
+  return 0;
+}
+// two_qubit_pauli_error_many: pairs (flat, k_flat even) in order, then the strategy if asked.
+int oracle_two_qubit_pauli_error(void* h, const uint32_t* pairs, size_t k_flat, const double* p,
+                                 int truncate) {
+  OSum* s = (OSum*)h;
+  if (k_flat % 2) return 1;
+  for (size_t i = 0; i < k_flat; i += 2)
+    if (pairs[i] >= s->n || pairs[i + 1] >= s->n || pairs[i] == pairs[i + 1]) return 1;
+  for (size_t i = 0; i < k_flat; i += 2) s->two_qubit_pauli_error(pairs[i], pairs[i + 1], p);
+  if (truncate) s->truncate();
   return 0;
 }
 int oracle_set_preserve(void* h, const uint64_t* x, const uint64_t* z, size_t k) {

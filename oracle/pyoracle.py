@@ -61,6 +61,8 @@ def lib():
         L.oracle_run_ops.restype = ctypes.c_int
         L.oracle_run_ops.argtypes = [vp, ctypes.POINTER(OpStruct), sz, P64]
         L.oracle_pauli_rotation.argtypes = [vp, P64, P64, dbl]
+        L.oracle_two_qubit_pauli_error.restype = ctypes.c_int
+        L.oracle_two_qubit_pauli_error.argtypes = [vp, ctypes.POINTER(u32), sz, PD, ctypes.c_int]
         L.oracle_overlap_with_zero.restype = dbl
         L.oracle_overlap_with_zero.argtypes = [vp]
         L.oracle_trace.restype = ctypes.c_int
@@ -145,6 +147,17 @@ class OracleSum:
         gx = np.ascontiguousarray(gx, dtype=np.uint64)
         gz = np.ascontiguousarray(gz, dtype=np.uint64)
         lib().oracle_pauli_rotation(self._h, _p64(gx), _p64(gz), theta)
+
+    def two_qubit_pauli_error(self, pairs_flat, p, truncate: bool = True):
+        """two_qubit_pauli_error_many over the flat pair list (noise.rs:39-105)."""
+        t = np.ascontiguousarray(pairs_flat, dtype=np.uint32)
+        pp = np.ascontiguousarray(p, dtype=np.float64)
+        if pp.shape != (15,):
+            raise ValueError("p needs 15 probabilities")
+        rc = lib().oracle_two_qubit_pauli_error(self._h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                                len(t), _pd(pp), 1 if truncate else 0)
+        if rc != 0:
+            raise ValueError("bad pair list")
 
     def overlap_with_zero(self) -> float:
         return lib().oracle_overlap_with_zero(self._h)

@@ -67,6 +67,8 @@ _SIGS = {
     "ppvm_pauli_error": [_P, _U32P, _SZ, _DP, _I],
     "ppvm_depolarize1": [_P, _U32P, _SZ, ctypes.c_double, _I],
     "ppvm_depolarize2": [_P, _U32P, _SZ, ctypes.c_double, _I],
+    "ppvm_two_qubit_pauli_error": [_P, _U32P, _SZ, _DP, _I],
+    "ppvm_amplitude_damping": [_P, ctypes.c_uint32, ctypes.c_double, _I],
     "ppvm_truncate": [_P],
     "ppvm_overlap_with_zero": [_P, _DP],
     "ppvm_expectation": [_P, _DP],

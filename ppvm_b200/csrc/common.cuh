@@ -27,6 +27,7 @@ struct Ctrl {
   double sum;                  // result slot of reductions
   unsigned long long umax;     // result slot of max reductions
   unsigned long long cap_needed;
+  unsigned long long fb_cut;   // fused-run fallback: 65536 - (gates of the longest run prefix that fits), 0 = none
 };
 
 // Per-op counters recorded for the term-gate-updates metric and the roofline bytes.

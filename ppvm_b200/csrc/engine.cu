@@ -25,6 +25,7 @@
 #include "runs.cuh"
 #include "tableau.cuh"
 #include "budget.cuh"
+#include "noise.cuh"
 
 using namespace ppvm;
 
@@ -129,12 +130,14 @@ struct ppvm_sum {
   RunScratch R = {};
   unsigned long long* tstate2 = nullptr;
   std::vector<int> swaps;      // op indices of fused runs enqueued in the current attempt
-  std::set<size_t> no_fuse;    // run starts that must take the per-gate path
+  std::map<size_t, int> run_cap;   // run start -> most gates a fused run there may take (1: per gate)
+  std::map<size_t, int> run_len;   // run start -> gates of the fused run enqueued there (this attempt)
   uint32_t* s_idx = nullptr;
   uint64_t* s_rec = nullptr;
   uint32_t* partner = nullptr;
   unsigned long long* table = nullptr;
   unsigned long long table_cap = 0;
+  unsigned long long run_slots_used = 0;  // group-table slots the fused runs since the last clean state hashed into
   unsigned long long* tstate = nullptr;
   unsigned long long tstate_cap = 0;
   uint64_t* side = nullptr;
@@ -150,6 +153,8 @@ struct ppvm_sum {
   SelState* d_sel = nullptr;   // radix select state of budget truncation
   unsigned* d_hist = nullptr;  // its digit histogram (2^11 bins, kept zero between uses)
   uint64_t* d_pres_keys = nullptr;
+  std::vector<double> perr2_host;    // factor tables of the internal two-qubit Pauli error ops
+  const double* d_perr2 = nullptr;   // their staged copy for the current attempt
   int* d_pres_table = nullptr;
   unsigned pres_mask = 0;
   int npres = 0;
@@ -275,7 +280,7 @@ void free_scratch(ppvm_sum* s) {
   pool_free(s->alt);
   pool_free(s->tstate2);
   uint32_t* run_arrays[] = {s->R.gslot, s->R.grp_min, s->R.grp_cnt, s->R.grp_ord, s->R.g_start,
-                            s->R.g_cnt, s->R.g_rep, s->R.g_fill, s->R.members};
+                            s->R.g_cnt, s->R.g_rep, s->R.g_fill, s->R.mcoord};
   for (uint32_t* p : run_arrays) pool_free(p);
   pool_free(s->R.created);
   s->R = RunScratch{};
@@ -293,11 +298,17 @@ void free_scratch(ppvm_sum* s) {
   s->tstate = nullptr;
 }
 
-// The fused-run group tables in their clean state (grp_min all ones, counts zero).
-ppvm_status clear_run_tables(ppvm_sum* s) {
-  CUDA_TRY(cudaMemsetAsync(s->R.grp_min, 0xFF, sizeof(uint32_t) * s->table_cap, s->stream));
-  CUDA_TRY(cudaMemsetAsync(s->R.grp_cnt, 0, sizeof(uint32_t) * s->table_cap, s->stream));
+// The fused-run group tables in their clean state (grp_min all ones, counts zero) over their
+// first `slots` entries: the whole table after allocation, and after a failed attempt only
+// the part its runs hashed into (a handle's table can be far larger than the sum it holds).
+ppvm_status clear_run_tables(ppvm_sum* s, unsigned long long slots) {
+  slots = std::min<unsigned long long>(slots, s->table_cap);
+  if (slots) {
+    CUDA_TRY(cudaMemsetAsync(s->R.grp_min, 0xFF, sizeof(uint32_t) * slots, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->R.grp_cnt, 0, sizeof(uint32_t) * slots, s->stream));
+  }
   CUDA_TRY(cudaMemsetAsync(s->R.created, 0, sizeof(unsigned long long) * kRunMaxGates, s->stream));
+  s->run_slots_used = 0;
   return PPVM_OK;
 }
 
@@ -340,9 +351,12 @@ ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   CUDA_TRY(pool_malloc((void**)&s->R.g_cnt, sizeof(uint32_t) * new_cap));
   CUDA_TRY(pool_malloc((void**)&s->R.g_rep, sizeof(uint32_t) * new_cap));
   CUDA_TRY(pool_malloc((void**)&s->R.g_fill, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.members, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->R.mcoord, sizeof(uint32_t) * new_cap));
+  // member coefficients and group keys live in the rotation records, unused during a run
+  s->R.mcoef = reinterpret_cast<double*>(s->s_rec);
+  s->R.gkey = s->s_rec + new_cap;  // 2W words per group, at most new_cap groups
   CUDA_TRY(pool_malloc((void**)&s->R.created, sizeof(unsigned long long) * kRunMaxGates));
-  return clear_run_tables(s);
+  return clear_run_tables(s, s->table_cap);
 }
 
 ppvm_status ensure_log(ppvm_sum* s, size_t nops) {
@@ -500,6 +514,10 @@ void prof_collect(ppvm_sum* s, const std::vector<int>& test_words) {
 }
 
 // ---- op lowering ----------------------------------------------------------------------------
+// Internal op code, never accepted in a public gate list: TwoQubitPauliError on (q0, q1) with
+// the factor table at perr2_host[16 * theta]; made only by ppvm_two_qubit_pauli_error.
+constexpr uint32_t kOpPauliError2 = 0x100;
+
 bool is_clifford_angle(const ppvm_sum* s, double th) {
   return (s->flags & PPVM_FLAG_CLIFFORD_ANGLES) && (th == kHalfPi || th == -kHalfPi);
 }
@@ -510,7 +528,8 @@ bool is_local(const ppvm_sum* s, const ppvm_op& op) {
     case PPVM_OP_RX: case PPVM_OP_RY: case PPVM_OP_RZ:
     case PPVM_OP_RXX: case PPVM_OP_RYY: case PPVM_OP_RZZ:
       return is_clifford_angle(s, op.theta);
-    case PPVM_OP_TRUNCATE: return false;
+    case PPVM_OP_TRUNCATE: case PPVM_OP_AMPLITUDE_DAMPING: return false;
+    case kOpPauliError2: return true;
     default: return op.code < PPVM_OP_COUNT_;
   }
 }
@@ -558,6 +577,7 @@ DevOp to_devop(const ppvm_op& op) {
     }
     case PPVM_OP_DEPOLARIZE1: d.code = C_DEP1; d.f0 = 1.0 - op.theta * (4.0 / 3.0); break;
     case PPVM_OP_DEPOLARIZE2: d.code = C_DEP2; d.f0 = 1.0 - op.theta * (16.0 / 15.0); break;
+    case kOpPauliError2: d.code = C_PERR2; d.f0 = op.theta; break;  // theta: factor table index
     default: {  // Clifford-angle rotation
       d.code = C_ROTC;
       const bool gx = op.code == PPVM_OP_RX || op.code == PPVM_OP_RY || op.code == PPVM_OP_RXX ||
@@ -712,11 +732,47 @@ struct K {
     s->n_ub = std::min<unsigned long long>(s->cap, 2 * s->n_ub);
   }
 
+  // AmplitudeDamping::amplitude_damping (noise.rs:132-163) on qubit q: see noise.cuh.
+  static void damping(ppvm_sum* s, uint32_t q, double gamma, int op) {
+    const Planes P = s->planes_view();
+    Gen g;
+    std::memset(&g, 0, sizeof(g));
+    g.gz[q >> 6] = 1ull << (q & 63);
+    const unsigned qmask = 1u << (q >> 6);
+    const double om = 1.0 - gamma;    // T::Coeff::from(1.0) - gamma
+    const double sxy = std::sqrt(om);  // (1 - gamma).sqrt()
+    const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
+    {
+      ProfScope ps(s, F_SCAN, op, 1);
+      launch(k_rot_scan<W, kScanBlock, ITEMS, true>, grid_for(nub, TILE, 8), kScanBlock, 0, s->stream,
+          P, s->d_ctrl, g, 0u, qmask, s->s_idx, s->s_rec, s->partner, s->tstate,
+          s->next_tile_epoch(), op, s->d_log);
+    }
+    const unsigned tep = s->next_table_epoch();
+    {
+      ProfScope ps(s, F_PAIR, op, 1);
+      launch(k_damp_index<W>, grid_for(nub, kPairBlock, 8), kPairBlock, 0, s->stream,
+          s->d_ctrl, g, s->s_rec, s->table, s->table_cap, tep, op);
+      launch(k_damp_probe<W>, grid_for(nub, kPairBlock, 8), kPairBlock, 0, s->stream,
+          P, s->d_ctrl, g, q >> 6, s->s_rec, s->partner, s->table, s->table_cap, tep, sxy, op);
+    }
+    {
+      ProfScope ps(s, F_APPLY, op, 1);
+      launch(k_damp_apply<W, kScanBlock, ITEMS>, grid_for(nub, TILE, 8), kScanBlock, 0, s->stream,
+          P, s->d_ctrl, g, om, gamma, s->s_idx, s->s_rec, s->partner, s->tstate, s->next_tile_epoch(), op);
+    }
+    {
+      ProfScope ps(s, F_COMMIT, op, 1);
+      launch(k_commit_damp, 1, 1, 0, s->stream, s->d_ctrl, op, s->d_log);
+    }
+    s->n_ub = std::min<unsigned long long>(s->cap, 2 * s->n_ub);
+  }
+
   static void clifford(ppvm_sum* s, const DevOp* ops_dev, int nops, int op0) {
     const Planes P = s->planes_view();
     ProfScope ps(s, F_CLIFF, op0, nops);
     launch(k_clifford<W, kCliffBlock>, grid_for(std::max<unsigned long long>(s->n_ub, 1), kCliffBlock, 16),
-           kCliffBlock, 0, s->stream, P, s->d_ctrl, ops_dev, nops, op0, s->d_log);
+           kCliffBlock, 0, s->stream, P, s->d_ctrl, ops_dev, nops, op0, s->d_log, s->d_perr2);
   }
 
   static void truncate(ppvm_sum* s, int op) {
@@ -739,6 +795,7 @@ struct K {
     const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
     unsigned long long tsize = next_pow2(std::max<unsigned long long>(2 * nub, 1024));
     if (tsize > s->table_cap) tsize = s->table_cap;
+    s->run_slots_used = std::max(s->run_slots_used, tsize);
     const void* d_rd_v = nullptr;
     PPVM_TRY(stage_put(s, &rd, sizeof(RunDesc), &d_rd_v));
     const RunDesc* d_rd = static_cast<const RunDesc*>(d_rd_v);
@@ -760,7 +817,7 @@ struct K {
     }
     {
       ProfScope ps(s, F_RUN_SCATTER, op0, L);
-      launch(k_run_scatter, grid_for(nub, 256, 8), 256, 0, s->stream, s->d_ctrl, s->R);
+      launch(k_run_scatter<W>, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, d_rd, s->R);
     }
     {
       ProfScope ps(s, F_RUN_GROUPS, op0, L);
@@ -922,6 +979,7 @@ ppvm_status clear_err(ppvm_sum* s) {
   Ctrl c = *s->h_ctrl;
   c.err = 0;
   c.err_op = 0;
+  c.fb_cut = 0;
   for (int t = 0; t < 4; ++t) c.tickets[t] = 0;
   CUDA_TRY(cudaMemcpyAsync(s->d_ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -935,6 +993,12 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
                     const std::vector<Gen>& gens, std::vector<int>& test_words) {
   std::vector<DevOp> run;  // pending local ops (Cliffords, Clifford-angle rotations, noise)
   int run_start = -1;
+  s->d_perr2 = nullptr;
+  if (!s->perr2_host.empty()) {
+    const void* d = nullptr;
+    PPVM_TRY(stage_put(s, s->perr2_host.data(), sizeof(double) * s->perr2_host.size(), &d));
+    s->d_perr2 = static_cast<const double*>(d);
+  }
   // in-place per-op pass over run[a, b)
   auto per_op = [&](size_t a, size_t b) -> ppvm_status {
     size_t off = a;
@@ -993,20 +1057,27 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
       if (!fused) DISPATCH_W(s->W, truncate(s, (int)i));
       continue;
     }
+    if (op.code == PPVM_OP_AMPLITUDE_DAMPING) {
+      PPVM_TRY(flush(-1, nullptr));
+      DISPATCH_W(s->W, damping(s, op.q0, op.theta, (int)i));
+      continue;
+    }
     if (is_local(s, op)) {
       if (run.empty()) run_start = (int)i;
       run.push_back(to_devop(op));
       continue;
     }
     // fused run of single-qubit RX (or RZ) rotations on distinct qubits
+    const auto cap_it = s->run_cap.find(i);
+    const int max_gates = cap_it == s->run_cap.end() ? kRunMaxGates : cap_it->second;
     const bool fusable = (op.code == PPVM_OP_RX || op.code == PPVM_OP_RZ) &&
-                         !(s->flags & PPVM_FLAG_EXACT_ORDER) && s->npres == 0 && !s->no_fuse.count(i);
+                         !(s->flags & PPVM_FLAG_EXACT_ORDER) && s->npres == 0 && max_gates >= 2;
     if (fusable) {
       RunDesc rd;
       std::memset(&rd, 0, sizeof(rd));
       rd.cls = op.code == PPVM_OP_RX ? 0 : 1;
       size_t j = i;
-      while (j < n_ops && (int)(j - i) < kRunMaxGates) {
+      while (j < n_ops && (int)(j - i) < max_gates) {
         const ppvm_op& o = ops[j];
         if (o.flags != 0 || o.code != op.code || is_clifford_angle(s, o.theta)) break;
         if ((rd.Q[o.q0 >> 6] >> (o.q0 & 63)) & 1ull) break;  // qubit repeats: end the run
@@ -1021,6 +1092,7 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
         PPVM_TRY(flush(-1, nullptr));
         const int trunc_op = (j < n_ops && ops[j].code == PPVM_OP_TRUNCATE && ops[j].flags == 0) ? (int)j : -1;
         PPVM_TRY(enqueue_run(s, rd, (int)i, (int)rd.L, trunc_op));
+        s->run_len[i] = (int)rd.L;
         i = trunc_op >= 0 ? j : j - 1;  // the loop's ++i moves past the run (and its TRUNCATE)
         continue;
       }
@@ -1043,9 +1115,13 @@ ppvm_status run_list(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, const std::v
   PPVM_TRY(ensure_log(s, std::max<size_t>(n_ops, 1)));
   std::vector<int> test_words(n_ops, 0);
   size_t start = 0;
-  s->no_fuse.clear();
-  for (int attempt = 0; attempt < 64; ++attempt) {
+  s->run_cap.clear();
+  // every failed attempt grows the capacity or cuts a run, so the loop ends; the bound only
+  // turns a logic error into a status
+  const size_t max_attempts = 64 + 8 * n_ops;
+  for (size_t attempt = 0; attempt < max_attempts; ++attempt) {
     s->swaps.clear();
+    s->run_len.clear();
     stage_reset(s);  // the stream is idle here: every earlier upload has completed
     PPVM_TRY(enqueue(s, ops, n_ops, start, gens, test_words));
     PPVM_TRY(sync_state(s, n_ops));
@@ -1058,13 +1134,20 @@ ppvm_status run_list(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, const std::v
       return PPVM_OK;
     }
     if (s->prof) prof_collect(s, test_words);
-    PPVM_TRY(clear_run_tables(s));  // a run stopped part-way leaves its slots set
+    PPVM_TRY(clear_run_tables(s, s->run_slots_used));  // a run stopped part-way leaves its slots set
     // fused runs at or after the failing op did not run: give their buffers back
     for (int op0 : s->swaps)
       if (op0 >= c.err_op) std::swap(s->planes, s->alt);
     if (c.err == kErrFallback && c.err_op >= 0 && (size_t)c.err_op >= start) {
+      // a group of the run starting at err_op has more than kRunMaxK coordinates: replay
+      // from there with the run cut to its longest prefix in which every term has at most
+      // kRunMaxK coordinates (reported by k_run_classify, at least kRunMaxK gates); the rest
+      // forms the next run
       start = (size_t)c.err_op;
-      s->no_fuse.insert(start);
+      const auto len = s->run_len.find(start);
+      int cut = c.fb_cut ? (int)(65536ull - c.fb_cut) : 1;
+      if (len != s->run_len.end() && cut >= len->second) cut = len->second / 2;  // not expected
+      s->run_cap[start] = std::max(cut, 1);
       PPVM_TRY(clear_err(s));
       s->n_ub = s->n_host;
       continue;
@@ -1227,7 +1310,8 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
     c->n_host = c->n_ub = 0;
     c->poisoned = false;
     c->swaps.clear();
-    c->no_fuse.clear();
+    c->run_cap.clear();
+    c->run_len.clear();
     c->npres = 0;
     c->h_pres.clear();
     c->prof = false;
@@ -1327,14 +1411,17 @@ void destroy_now(ppvm_sum* s) {
 }
 
 ppvm_sum* take_cached(int device, int W) {
+  // the largest cached capacity: a new sum then rarely grows (growth replays ops)
   std::lock_guard<std::mutex> lk(g_pool_mu);
+  long best = -1;
   for (size_t i = 0; i < g_sum_cache.size(); ++i)
-    if (g_sum_cache[i]->device == device && g_sum_cache[i]->W == W) {
-      ppvm_sum* s = g_sum_cache[i];
-      g_sum_cache.erase(g_sum_cache.begin() + (long)i);
-      return s;
-    }
-  return nullptr;
+    if (g_sum_cache[i]->device == device && g_sum_cache[i]->W == W &&
+        (best < 0 || g_sum_cache[i]->cap > g_sum_cache[(size_t)best]->cap))
+      best = (long)i;
+  if (best < 0) return nullptr;
+  ppvm_sum* s = g_sum_cache[(size_t)best];
+  g_sum_cache.erase(g_sum_cache.begin() + best);
+  return s;
 }
 }  // namespace
 
@@ -1638,6 +1725,71 @@ ppvm_status ppvm_depolarize1(ppvm_sum* s, const uint32_t* t, size_t k, double p,
 }
 ppvm_status ppvm_depolarize2(ppvm_sum* s, const uint32_t* t, size_t k, double p, int truncate) {
   return run_gate(s, PPVM_OP_DEPOLARIZE2, t, k, true, p, nullptr, truncate);
+}
+
+// The factor of each (P_a, P_b), code x | z << 1 per qubit, is 1 - 2 p[i1] - ... - 2 p[i8] over
+// the eight two-qubit Paulis that anticommute with it, subtracted in the order the reference
+// writes them (noise.rs:50-99; the order fixes the rounding).  p indices name IX IY IZ XI XX
+// XY XZ YI YX YY YZ ZI ZX ZY ZZ.
+static void perr2_factors(const double p[15], double f[16]) {
+  static const int8_t kOrder[16][8] = {
+      {0},                              // II: unchanged
+      {1, 10, 13, 14, 2, 5, 6, 9},      // IX
+      {0, 1, 12, 13, 4, 5, 8, 9},       // IZ
+      {0, 10, 12, 14, 2, 4, 6, 8},      // IY
+      {10, 11, 12, 13, 14, 7, 8, 9},    // XI
+      {1, 11, 12, 2, 5, 6, 7, 8},       // XX
+      {0, 1, 10, 11, 14, 4, 5, 7},      // XZ
+      {0, 11, 13, 2, 4, 6, 7, 9},       // XY
+      {10, 3, 4, 5, 6, 7, 8, 9},        // ZI
+      {1, 13, 14, 2, 3, 4, 7, 8},       // ZX
+      {0, 1, 10, 12, 13, 3, 6, 7},      // ZZ
+      {0, 12, 14, 2, 3, 5, 7, 9},       // ZY
+      {11, 12, 13, 14, 3, 4, 5, 6},     // YI
+      {1, 10, 11, 12, 2, 3, 4, 9},      // YX
+      {0, 1, 11, 14, 3, 6, 8, 9},       // YZ
+      {0, 10, 11, 13, 2, 3, 5, 8}};     // YY
+  f[0] = 1.0;
+  for (int code = 1; code < 16; ++code) {
+    double acc = 1.0;
+    for (int t = 0; t < 8; ++t) acc = acc - p[kOrder[code][t]] * 2.0;
+    f[code] = acc;
+  }
+}
+
+ppvm_status ppvm_two_qubit_pauli_error(ppvm_sum* s, const uint32_t* t, size_t k, const double p[15],
+                                       int truncate) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  if (!p || (k && !t)) return fail(PPVM_EINVAL, "null argument");
+  if (k % 2) return fail(PPVM_EINVAL, "two-qubit operations require an even number of targets");
+  std::vector<ppvm_op> ops;
+  for (size_t i = 0; i < k; i += 2) {
+    if (t[i] >= s->n || t[i + 1] >= s->n || t[i] == t[i + 1])
+      return fail(PPVM_EINVAL, "two-qubit op needs two distinct qubits in range");
+    ppvm_op op;
+    std::memset(&op, 0, sizeof(op));
+    op.code = kOpPauliError2;
+    op.q0 = t[i];
+    op.q1 = t[i + 1];
+    op.theta = 0.0;  // every pair of the call uses table 0
+    ops.push_back(op);
+  }
+  if (truncate) {
+    ppvm_op op;
+    std::memset(&op, 0, sizeof(op));
+    op.code = PPVM_OP_TRUNCATE;
+    ops.push_back(op);
+  }
+  if (ops.empty()) return PPVM_OK;
+  s->perr2_host.assign(16, 0.0);
+  perr2_factors(p, s->perr2_host.data());
+  const ppvm_status st = run_list(s, ops.data(), ops.size(), {});
+  s->perr2_host.clear();
+  return st;
+}
+
+ppvm_status ppvm_amplitude_damping(ppvm_sum* s, uint32_t q, double gamma, int truncate) {
+  return run_gate(s, PPVM_OP_AMPLITUDE_DAMPING, &q, 1, false, gamma, nullptr, truncate);
 }
 
 ppvm_status ppvm_pauli_rotation(ppvm_sum* s, const uint64_t* gx, const uint64_t* gz, double theta, int truncate) {

@@ -58,8 +58,10 @@ struct ItemsFor {
 
 // ---------------------------------------------------------------------------------------
 // k_rot_scan: flags anticommuting terms, writes their index and record in index order.
+// With DAMP the flagged terms are those with Z (x = 0, z = 1) on the qubit of g.gz instead:
+// the parents of amplitude damping.
 // ---------------------------------------------------------------------------------------
-template <int W, int BLOCK, int ITEMS>
+template <int W, int BLOCK, int ITEMS, bool DAMP = false>
 __global__ void __launch_bounds__(BLOCK)
 k_rot_scan(Planes P, Ctrl* ctrl, Gen g, unsigned xmask, unsigned zmask, uint32_t* s_idx, uint64_t* s_rec,
            uint32_t* partner, unsigned long long* ts, unsigned epoch, int op, OpLog* log) {
@@ -92,12 +94,20 @@ k_rot_scan(Planes P, Ctrl* ctrl, Gen g, unsigned xmask, unsigned zmask, uint32_t
       bool a = false;
       if (i < N) {
         uint64_t acc = 0;
+        if constexpr (DAMP) {
 #pragma unroll
-        for (int w = 0; w < W; ++w) {
-          if ((xmask >> w) & 1u) acc ^= P.x[(unsigned long long)w * P.cap + i] & g.gz[w];
-          if ((zmask >> w) & 1u) acc ^= P.z[(unsigned long long)w * P.cap + i] & g.gx[w];
+          for (int w = 0; w < W; ++w)
+            if ((zmask >> w) & 1u)
+              acc |= P.z[(unsigned long long)w * P.cap + i] & ~P.x[(unsigned long long)w * P.cap + i] & g.gz[w];
+          a = acc != 0;
+        } else {
+#pragma unroll
+          for (int w = 0; w < W; ++w) {
+            if ((xmask >> w) & 1u) acc ^= P.x[(unsigned long long)w * P.cap + i] & g.gz[w];
+            if ((zmask >> w) & 1u) acc ^= P.z[(unsigned long long)w * P.cap + i] & g.gx[w];
+          }
+          a = __popcll(acc) & 1;
         }
-        a = __popcll(acc) & 1;
       }
       ballots[k] = __ballot_sync(kFull, a);
     }
@@ -418,7 +428,8 @@ enum CliffCode : uint32_t {
   C_X = 0, C_Y, C_Z, C_H, C_S, C_SDAG, C_SQX, C_SQXDAG, C_SQY, C_SQYDAG,
   C_CNOT, C_CZ, C_CY,
   C_PAULI_ERROR, C_DEP1, C_DEP2,
-  C_ROTC  // Clifford-angle rotation on 1-2 qubits: axis bits in ax/az, sign of sin in f0
+  C_ROTC,  // Clifford-angle rotation on 1-2 qubits: axis bits in ax/az, sign of sin in f0
+  C_PERR2  // two-qubit Pauli error: factor table f0 (16 doubles each) of the launch's tables
 };
 
 struct DevOp {
@@ -434,7 +445,8 @@ constexpr int kCliffBlock = 128;
 
 template <int W, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
-k_clifford(Planes P, Ctrl* ctrl, const DevOp* ops, int nops, int op0, OpLog* log) {
+k_clifford(Planes P, Ctrl* ctrl, const DevOp* ops, int nops, int op0, OpLog* log,
+           const double* __restrict__ perr2) {
   pdl_wait();
   __shared__ DevOp s_ops[kMaxOpsPerLaunch];
   __shared__ uint64_t s_x[W][BLOCK];
@@ -520,6 +532,12 @@ k_clifford(Planes P, Ctrl* ctrl, const DevOp* ops, int nops, int op0, OpLog* log
           break;
         }
         case C_DEP1: if (x0 | z0) c = __dmul_rn(c, d.f0); break;
+        case C_PERR2: {  // factor of (P_q0, P_q1), code x | z << 1 on each qubit
+          const bool x1 = s_x[d.w1][t] & m1, z1 = s_z[d.w1][t] & m1;
+          const int code = ((int)x0 | ((int)z0 << 1)) << 2 | (int)x1 | ((int)z1 << 1);
+          if (code) c = __dmul_rn(c, perr2[16 * (int)d.f0 + code]);
+          break;
+        }
         case C_DEP2: {
           const bool x1 = s_x[d.w1][t] & m1, z1 = s_z[d.w1][t] & m1;
           if (x0 | z0 | x1 | z1) c = __dmul_rn(c, d.f0);

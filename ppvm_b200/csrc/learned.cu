@@ -89,35 +89,38 @@ __global__ void k_mlp_pack(const float* p, MlpWeights* w) {
   if (threadIdx.x == 0) w->b3 = p[kOffB3];
 }
 
-// Adam on the flat parameter vector, gradients cleared, then the device weights repacked.
-__global__ void k_mlp_adam(float* p, float* m, float* v, float* g, MlpWeights* w, float lr_t, float b1, float b2,
-                           float eps) {
-  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
-    const float gi = g[i];
-    const float mi = b1 * m[i] + (1.0f - b1) * gi;
-    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    p[i] -= lr_t * mi / (sqrtf(vi) + eps);
-    g[i] = 0.0f;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < kMlpH * kMlpK1; i += blockDim.x) {
-    const int n = i / kMlpK1, k = i % kMlpK1;
-    w->w1[i] = __float2bfloat16_rn(k < kMlpIn ? p[kOffW1 + n * kMlpIn + k] : 0.0f);
-  }
-  for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x) {
-    const int n = i / kMlpH, k = i % kMlpH;
-    const __nv_bfloat16 b = __float2bfloat16_rn(p[kOffW2 + i]);
-    w->w2[i] = b;
+// Adam on the flat parameter vector, one thread per parameter: the update, the gradient
+// cleared, and the parameter's own packed copies written (W1's zero padding is set once by
+// k_mlp_pack), so no thread waits for another.
+__global__ void __launch_bounds__(256) k_mlp_adam(float* p, float* m, float* v, float* g, MlpWeights* w, float lr_t,
+                                                  float b1, float b2, float eps) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kMlpParams) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float pi = p[i] - lr_t * mi / (sqrtf(vi) + eps);
+  p[i] = pi;
+  g[i] = 0.0f;
+  if (i < kOffB1) {
+    const int n = (i - kOffW1) / kMlpIn, k = (i - kOffW1) % kMlpIn;
+    w->w1[n * kMlpK1 + k] = __float2bfloat16_rn(pi);
+  } else if (i < kOffW2) {
+    w->b1[i - kOffB1] = pi;
+  } else if (i < kOffB2) {
+    const int n = (i - kOffW2) / kMlpH, k = (i - kOffW2) % kMlpH;
+    const __nv_bfloat16 b = __float2bfloat16_rn(pi);
+    w->w2[n * kMlpH + k] = b;
     w->w2t[k * kMlpH + n] = b;
+  } else if (i < kOffW3) {
+    w->b2[i - kOffB2] = pi;
+  } else if (i < kOffB3) {
+    w->w3[i - kOffW3] = pi;
+  } else {
+    w->b3 = pi;
   }
-  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-    w->b1[i] = p[kOffB1 + i];
-    w->b2[i] = p[kOffB2 + i];
-    w->w3[i] = p[kOffW3 + i];
-  }
-  if (threadIdx.x == 0) w->b3 = p[kOffB3];
 }
 
 // Stages the features of rows [r0, r0+16) of the sample list into a BF16 [16][16] tile.
@@ -512,7 +515,8 @@ ppvm_status ppvm_mlp_train(ppvm_mlp* m, const float* feats, const float* targets
       MTRY(launch_train(m, true, st, cnt, 1.0f / (float)cnt));
       ++m->step;
       const float lr_t = lr * std::sqrt(1.0f - std::pow(b2, (float)m->step)) / (1.0f - std::pow(b1, (float)m->step));
-      k_mlp_adam<<<1, 256, 0, m->stream>>>(m->params, m->m, m->v, m->grads, m->w, lr_t, b1, b2, eps);
+      k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, m->stream>>>(m->params, m->m, m->v, m->grads, m->w, lr_t,
+                                                                   b1, b2, eps);
       MCUDA(cudaGetLastError());
     }
     MCUDA(cudaMemcpyAsync(&ls, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));

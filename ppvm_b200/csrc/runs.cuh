@@ -48,7 +48,9 @@ struct RunScratch {
   uint32_t* g_cnt;
   uint32_t* g_rep;
   uint32_t* g_fill;
-  uint32_t* members;
+  uint32_t* mcoord;    // per member, in group order: its coordinate index (bits of f at M)
+  double* mcoef;       // per member, in group order: its coefficient
+  uint64_t* gkey;      // per group: v[W] then f outside the coordinates, f0[W]
   unsigned long long* created;  // per gate of the run: children created
 };
 
@@ -77,7 +79,9 @@ k_run_classify(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, 
   __shared__ unsigned long long s_slot;
   __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
   __shared__ int s_err;
+  __shared__ uint16_t s_gidx[64 * W];  // qubit -> its gate's index in the run
   if (threadIdx.x == 0) s_err = ld_volatile_int(&ctrl->err);
+  for (unsigned j = threadIdx.x; j < rd->L; j += BLOCK) s_gidx[rd->q[j]] = (uint16_t)j;
   __syncthreads();
   if (s_err) return;
   const unsigned long long N = ld_volatile(&ctrl->n);
@@ -122,6 +126,27 @@ k_run_classify(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, 
             if (wcap) keep = keep && (weight<W>(kx[it], kz[it]) <= maxw);
           }
         } else if (k > (unsigned)kRunMaxK) {
+          // the run's first g gates, g = the gate index of this term's (kRunMaxK+1)-th
+          // coordinate in gate order, hold at most kRunMaxK of its coordinates: the host
+          // cuts the run at the smallest such g over all terms (g >= kRunMaxK)
+          unsigned lo[kRunMaxK + 1];
+          unsigned nlo = 0;
+#pragma unroll
+          for (int w = 0; w < W; ++w) {
+            uint64_t m = M[w];
+            while (m) {
+              unsigned gi = s_gidx[w * 64 + (__ffsll((long long)m) - 1)];
+              m &= m - 1;
+              if (nlo == kRunMaxK + 1 && gi >= lo[kRunMaxK]) continue;
+              unsigned r = nlo < kRunMaxK + 1 ? nlo++ : kRunMaxK;
+              while (r > 0 && lo[r - 1] > gi) {
+                lo[r] = lo[r - 1];
+                --r;
+              }
+              lo[r] = gi;
+            }
+          }
+          atomicMax(&ctrl->fb_cut, 65536ull - lo[kRunMaxK]);
           set_err(ctrl, kErrFallback, op);
           R.gslot[i] = kNone;
         } else {
@@ -269,20 +294,52 @@ k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long lo
   }
 }
 
-// Also hands the group table back clean: grp_min and grp_cnt were last read by k_run_order,
-// so every member resets its slot (same values from every member), and the next run needs
-// no clearing pass.  After a device error the host clears both arrays instead.
-static __global__ void __launch_bounds__(256) k_run_scatter(Ctrl* ctrl, RunScratch R) {
+// Lays out each group's members contiguously, as (coordinate index, coefficient) records,
+// and the group's key (from its representative), so k_run_groups reads one span per group
+// instead of gathering members by index.  A member's coordinate index has bit t set when f
+// has a 1 at the t-th lowest qubit of M = v & Q (the order k_run_groups uses).  Also hands
+// the group table back clean: grp_min and grp_cnt were last read by k_run_order, so every
+// member resets its slot (same values from every member), and the next run needs no
+// clearing pass.  After a device error the host clears both arrays instead.
+template <int W>
+__global__ void __launch_bounds__(256) k_run_scatter(Planes P, Ctrl* ctrl, const RunDesc* rd, RunScratch R) {
   pdl_wait();
   if (ld_volatile_int(&ctrl->err)) return;
   const unsigned long long N = ld_volatile(&ctrl->n);
+  const uint32_t cls = rd->cls;
+  uint64_t Q[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) Q[w] = rd->Q[w];
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
        i += (unsigned long long)gridDim.x * blockDim.x) {
     const uint32_t s = R.gslot[i];
     if (s == kNone) continue;
     const uint32_t o = R.grp_ord[s];
     const uint32_t pos = R.g_start[o] + atomicAdd(&R.g_fill[o], 1u);
-    R.members[pos] = (uint32_t)i;
+    uint64_t x[W], z[W], v[W], f[W];
+    load_key<W>(P, i, x, z);
+    split_planes<W>(cls, x, z, v, f);
+    unsigned c = 0, t = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      uint64_t m = v[w] & Q[w];
+      while (m) {
+        const int b = __ffsll((long long)m) - 1;
+        c |= (unsigned)((f[w] >> b) & 1ull) << t;
+        ++t;
+        m &= m - 1;
+      }
+    }
+    R.mcoord[pos] = c;
+    R.mcoef[pos] = P.c[i];
+    if (R.g_rep[o] == (uint32_t)i) {
+      uint64_t* gk = R.gkey + (unsigned long long)o * 2 * W;
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        gk[w] = v[w];
+        gk[W + w] = f[w] & ~(v[w] & Q[w]);
+      }
+    }
     R.grp_min[s] = kNone;
     R.grp_cnt[s] = 0u;
   }
@@ -331,15 +388,14 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
     unsigned k = 0;
     uint16_t pos[kRunMaxK];  // qubit of coordinate bit t (ascending)
     bool wok = true;
+    const uint32_t start = R.g_start[g], cnt = R.g_cnt[g];  // loaded beside the group key
     {
-      const uint32_t rep = R.g_rep[g];
-      uint64_t x[W], z[W], f[W];
-      load_key<W>(P, rep, x, z);
-      split_planes<W>(cls, x, z, v, f);
+      const uint64_t* gk = R.gkey + g * 2 * W;
 #pragma unroll
       for (int w = 0; w < W; ++w) {
+        v[w] = gk[w];
+        f0[w] = gk[W + w];
         M[w] = v[w] & rd->Q[w];
-        f0[w] = f[w] & ~M[w];
       }
 #pragma unroll
       for (int w = 0; w < W; ++w) {
@@ -352,15 +408,14 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
       }
     }
     const unsigned size = 1u << k;
-    if (lane == 0) {  // coordinate bits sorted by the position of their gate in the run
-      for (unsigned t = 0; t < k; ++t) {
-        unsigned r = t;
-        while (r > 0 && s_gidx[pos[s_ord[warp][r - 1]]] > s_gidx[pos[t]]) {
-          s_ord[warp][r] = s_ord[warp][r - 1];
-          --r;
-        }
-        s_ord[warp][r] = (uint8_t)t;
-      }
+    {  // coordinate bits sorted by the position of their gate in the run (distinct): lane t
+       // takes bit t, its rank is the number of bits whose gate comes earlier
+      unsigned key = 0xFFFFu;
+      for (unsigned t = 0; t < k; ++t)
+        if (t == lane) key = s_gidx[pos[t]];
+      unsigned rank = 0;
+      for (unsigned t = 0; t < k; ++t) rank += __shfl_sync(kFull, key, t) < key;
+      if (lane < k) s_ord[warp][rank] = (uint8_t)lane;
     }
     if (wcap) {
       unsigned wt = 0;
@@ -370,24 +425,9 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
     }
     for (unsigned e = lane; e < (size + 31) / 32; e += 32) ex[e] = 0u;
     __syncwarp();
-    const uint32_t start = R.g_start[g], cnt = R.g_cnt[g];
     for (uint32_t m = lane; m < cnt; m += 32) {
-      const uint32_t i = R.members[start + m];
-      uint64_t fw[W];
-#pragma unroll
-      for (int w = 0; w < W; ++w)
-        fw[w] = (M[w] != 0) ? (cls == 0 ? P.x[(unsigned long long)w * P.cap + i]
-                                        : P.z[(unsigned long long)w * P.cap + i])
-                            : 0ull;
-      unsigned c = 0;
-      for (unsigned t = 0; t < k; ++t) {
-        const unsigned q = pos[t];
-        uint64_t word = 0;
-#pragma unroll
-        for (int w = 0; w < W; ++w) word = (w == (int)(q >> 6)) ? fw[w] : word;
-        c |= (unsigned)((word >> (q & 63)) & 1ull) << t;
-      }
-      coef[c] = P.c[i];
+      const unsigned c = R.mcoord[start + m];
+      coef[c] = R.mcoef[start + m];
       atomicOr(&ex[c >> 5], 1u << (c & 31));
     }
     __syncwarp();

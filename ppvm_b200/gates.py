@@ -20,13 +20,14 @@ RX, RY, RZ = 13, 14, 15
 RXX, RYY, RZZ = 16, 17, 18
 PAULI_ERROR, DEPOLARIZE1, DEPOLARIZE2 = 19, 20, 21
 TRUNCATE = 22
+AMPLITUDE_DAMPING = 23
 
 NAMES = {
     X: "x", Y: "y", Z: "z", H: "h", S: "s", S_DAG: "s_dag", SQRT_X: "sqrt_x",
     SQRT_X_DAG: "sqrt_x_dag", SQRT_Y: "sqrt_y", SQRT_Y_DAG: "sqrt_y_dag", CNOT: "cnot",
     CZ: "cz", CY: "cy", RX: "rx", RY: "ry", RZ: "rz", RXX: "rxx", RYY: "ryy", RZZ: "rzz",
     PAULI_ERROR: "pauli_error", DEPOLARIZE1: "depolarize1", DEPOLARIZE2: "depolarize2",
-    TRUNCATE: "truncate",
+    TRUNCATE: "truncate", AMPLITUDE_DAMPING: "amplitude_damping",
 }
 SINGLE_CLIFFORD = {X, Y, Z, H, S, S_DAG, SQRT_X, SQRT_X_DAG, SQRT_Y, SQRT_Y_DAG}
 TWO_CLIFFORD = {CNOT, CZ, CY}
@@ -55,6 +56,10 @@ def r2(code: int, a: int, b: int, theta: float):
 
 def pauli_error(q: int, p):
     return (PAULI_ERROR, q, 0, 0.0, tuple(float(v) for v in p))
+
+
+def amplitude_damping(q: int, gamma: float):
+    return (AMPLITUDE_DAMPING, q, 0, float(gamma), _ZERO3)
 
 
 def truncate():

@@ -333,6 +333,24 @@ class PauliSum:
         arr, k = _u32(targets)
         self._check(lib().ppvm_depolarize2(self._h, arr, k, float(p), int(bool(truncate))))
 
+    def two_qubit_pauli_error(self, *a, p=None, truncate: bool = True):
+        """``two_qubit_pauli_error(targets, p, truncate=True)``: flat pair list, 15
+        probabilities of IX IY IZ XI XX XY XZ YI YX YY YZ ZI ZX ZY ZZ (noise.rs:39-105)."""
+        targets, p, truncate = _targets_value(a, p, "p", truncate)
+        pv = [float(v) for v in p]
+        if len(pv) != 15:
+            raise ValueError("two_qubit_pauli_error needs 15 probabilities")
+        arr, k = _u32(targets)
+        pp = (ctypes.c_double * 15)(*pv)
+        self._check(lib().ppvm_two_qubit_pauli_error(self._h, arr, k, pp, int(bool(truncate))))
+
+    def amplitude_damping(self, addr0: int, gamma: float, truncate: bool = True):
+        """Amplitude damping of qubit ``addr0`` (noise.rs:132-163): Z -> (1-g) Z + g I,
+        X/Y -> sqrt(1-g) X/Y."""
+        if int(addr0) < 0:
+            raise ValueError("qubit index out of range")
+        self._check(lib().ppvm_amplitude_damping(self._h, int(addr0), float(gamma), int(bool(truncate))))
+
     # ---- gate lists ------------------------------------------------------------------------------
     def run(self, ops) -> None:
         """Runs a gate list (``ppvm_b200.gates`` tuples, or a ``GateList`` built once with

@@ -60,6 +60,25 @@ def test_training_fits_a_smooth_target():
     assert after < 0.05 * before and after < 0.02, (before, after)
 
 
+def test_adam_step_and_repacked_weights():
+    """One full-batch step: Adam's first update is -lr * sign(g) (bias-corrected moments), and
+    the packed tensor-core weights follow the updated FP32 parameters."""
+    net, rng = rand_net(4)
+    X = rng.normal(0, 1, (1024, 8)).astype(np.float32)
+    t = rng.normal(0, 1, 1024).astype(np.float32)
+    p0 = net.params.astype(np.float64)
+    g, _ = net.grad(X, t)
+    lr = 1e-3
+    net.train(X, t, epochs=1, batch=len(t), lr=lr, seed=0)
+    p1 = net.params.astype(np.float64)
+    big = np.abs(g) > 1e-3  # eps = 1e-8 is negligible against sqrt(v) = 0.0316 |g|
+    assert big.sum() > 0.5 * len(g)
+    np.testing.assert_allclose(p1[big] - p0[big], -lr * np.sign(g[big]), rtol=1e-3, atol=1e-8)
+    y = net.predict(X)
+    want, _ = M.forward(p1, X, tc=True)
+    assert np.max(np.abs(y - want) / (1 + np.abs(want))) < 1e-2
+
+
 def _sum_after(L=5, layers=3):
     wl = C.kicked_ising_random_h(L=L, layers=layers, seed=5, thr=1e-7, obs=(L // 2, L // 2))
     s = PauliSum([wl.observable[0][0]], wl.n_qubits, [1.0], min_abs_coeff=1e-7, clifford_angles=True)

@@ -201,6 +201,24 @@ def test_capacity_growth_replay():
         assert len(g) > 4096
 
 
+def test_wide_run_splits_until_it_fits():
+    # Z on qubits 0..11 meets a 40-gate RX run in qubit order: 12 > 10 coordinates, so the
+    # run is cut where that term's 11th coordinate comes (10 gates) and the rest fuses as a
+    # second run; the RZ and RX layers after it cut again on a larger sum
+    n = 40
+    rng = np.random.default_rng(7)
+    terms = {"Z" * 12 + "I" * (n - 12): 1.0}
+    for _ in range(30):
+        w = ["I"] * n
+        for q in rng.choice(n, 4, replace=False):
+            w[int(q)] = "XYZ"[int(rng.integers(3))]
+        terms["".join(w)] = float(rng.uniform(-1, 1))
+    ops = [G.r1(G.RX, q, 0.4) for q in range(n)] + [G.truncate()]
+    ops += [G.r1(G.RZ, q, 0.3) for q in range(n)] + [G.truncate()]
+    ops += [G.r1(G.RX, q, -0.2) for q in range(n)] + [G.truncate()]
+    run_both(list(terms.items()), n, ops, thr=1e-6, check_every=n + 1, exact=False)
+
+
 @pytest.mark.parametrize("exact", [True, False])
 def test_tfim_config1_every_half(exact):
     wl = C.tfim_1d()
