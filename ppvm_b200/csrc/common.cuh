@@ -27,7 +27,8 @@ struct Ctrl {
   double sum;                  // result slot of reductions
   unsigned long long umax;     // result slot of max reductions
   unsigned long long cap_needed;
-  unsigned long long fb_cut;   // fused-run fallback: 65536 - (gates of the longest run prefix that fits), 0 = none
+  unsigned long long fb_cut;   // fused-run fallback: gates at the head of the run to apply one at a time, 0 = none
+  unsigned long long done;     // blocks of the current launch that finished (last_block_done)
 };
 
 // Per-op counters recorded for the term-gate-updates metric and the roofline bytes.
@@ -76,6 +77,23 @@ __device__ __forceinline__ void pdl_wait() {
   // Let the next kernel of the stream be launched now: it is scheduled only once every block
   // of this grid has started, and its blocks wait in their own pdl_wait() for this grid.
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// True (in every thread) in the last block of the grid to call it: by then every block's
+// writes made before its call are visible.  Blocks never wait on each other.  The last block
+// resets the counter for the next launch; after a device error the host resets it.
+__device__ __forceinline__ bool last_block_done(unsigned long long* counter) {
+  __shared__ bool s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned long long prev = atomicAdd(counter, 1ull);
+    s_last = prev == (unsigned long long)gridDim.x * gridDim.y * gridDim.z - 1;
+    if (s_last) *counter = 0;
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last;
 }
 
 __device__ __forceinline__ void set_err(Ctrl* ctrl, int code, int op) {

@@ -130,7 +130,7 @@ struct ppvm_sum {
   RunScratch R = {};
   unsigned long long* tstate2 = nullptr;
   std::vector<int> swaps;      // op indices of fused runs enqueued in the current attempt
-  std::map<size_t, int> run_cap;   // run start -> most gates a fused run there may take (1: per gate)
+  std::map<size_t, int> run_cap;   // run start -> most gates a fused run there may take; -L: L gates per gate
   std::map<size_t, int> run_len;   // run start -> gates of the fused run enqueued there (this attempt)
   uint32_t* s_idx = nullptr;
   uint64_t* s_rec = nullptr;
@@ -822,11 +822,8 @@ struct K {
     {
       ProfScope ps(s, F_RUN_GROUPS, op0, L);
       launch(k_run_groups<W>, grid_for(nub, kRunWarps, 8), kRunWarps * 32, 0, s->stream,
-          P, O, s->d_ctrl, d_rd, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0);
-    }
-    {
-      ProfScope ps(s, F_RUN_COMMIT, op0, L);
-      launch(k_run_commit, 1, kRunMaxGates, 0, s->stream, s->d_ctrl, s->R, op0, L, trunc_op, s->d_log);
+          P, O, s->d_ctrl, d_rd, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0,
+          trunc_op, s->d_log);  // its last block publishes the counts and the op log
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);
@@ -857,11 +854,8 @@ struct K {
       ProfScope ps(s, F_TABLEAU, op0, nops, trunc_op);
       launch(k_tableau<W, kTabBlock, ITEMS>, grid_for(nub, (unsigned long long)kTabBlock * ITEMS, bps), kTabBlock, smem, s->stream,
           P, O, s->d_ctrl, t.tp, static_cast<const uint64_t*>(d_rows), static_cast<const uint8_t*>(d_ph),
-          trunc_op >= 0 ? 1 : 0, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0, nops, s->d_log);
-    }
-    {
-      ProfScope ps(s, F_COMMIT, op0, nops);
-      launch(k_commit_tableau, 1, 1, 0, s->stream, s->d_ctrl, trunc_op, s->d_log);
+          trunc_op >= 0 ? 1 : 0, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0, nops, trunc_op,
+          s->d_log);  // its last block publishes the count
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);
@@ -980,6 +974,7 @@ ppvm_status clear_err(ppvm_sum* s) {
   c.err = 0;
   c.err_op = 0;
   c.fb_cut = 0;
+  c.done = 0;  // blocks that returned early on the error never counted
   for (int t = 0; t < 4; ++t) c.tickets[t] = 0;
   CUDA_TRY(cudaMemcpyAsync(s->d_ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -993,6 +988,7 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
                     const std::vector<Gen>& gens, std::vector<int>& test_words) {
   std::vector<DevOp> run;  // pending local ops (Cliffords, Clifford-angle rotations, noise)
   int run_start = -1;
+  size_t per_gate_end = 0;  // ops before this index take the per-gate path (a wide run)
   s->d_perr2 = nullptr;
   if (!s->perr2_host.empty()) {
     const void* d = nullptr;
@@ -1069,9 +1065,14 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
     }
     // fused run of single-qubit RX (or RZ) rotations on distinct qubits
     const auto cap_it = s->run_cap.find(i);
-    const int max_gates = cap_it == s->run_cap.end() ? kRunMaxGates : cap_it->second;
+    int max_gates = cap_it == s->run_cap.end() ? kRunMaxGates : cap_it->second;
+    if (max_gates < 0) {  // the run starting here goes gate by gate: -max_gates gates
+      per_gate_end = i + (size_t)(-max_gates);
+      max_gates = 0;
+    }
     const bool fusable = (op.code == PPVM_OP_RX || op.code == PPVM_OP_RZ) &&
-                         !(s->flags & PPVM_FLAG_EXACT_ORDER) && s->npres == 0 && max_gates >= 2;
+                         !(s->flags & PPVM_FLAG_EXACT_ORDER) && s->npres == 0 && max_gates >= 2 &&
+                         i >= per_gate_end;
     if (fusable) {
       RunDesc rd;
       std::memset(&rd, 0, sizeof(rd));
@@ -1139,15 +1140,16 @@ ppvm_status run_list(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, const std::v
     for (int op0 : s->swaps)
       if (op0 >= c.err_op) std::swap(s->planes, s->alt);
     if (c.err == kErrFallback && c.err_op >= 0 && (size_t)c.err_op >= start) {
-      // a group of the run starting at err_op has more than kRunMaxK coordinates: replay
-      // from there with the run cut to its longest prefix in which every term has at most
-      // kRunMaxK coordinates (reported by k_run_classify, at least kRunMaxK gates); the rest
-      // forms the next run
+      // a group of the run starting at err_op has more than kRunMaxK coordinates.  A
+      // group's coordinates are fixed for the whole run (the plane the gates leave alone
+      // holds them), so k_run_classify reports the number p of leading gates after which
+      // every term, and every descendant, has at most kRunMaxK coordinates left.  Replay
+      // with those p gates one at a time and the rest as one fused run, which then fits.
       start = (size_t)c.err_op;
       const auto len = s->run_len.find(start);
-      int cut = c.fb_cut ? (int)(65536ull - c.fb_cut) : 1;
-      if (len != s->run_len.end() && cut >= len->second) cut = len->second / 2;  // not expected
-      s->run_cap[start] = std::max(cut, 1);
+      const int L = len == s->run_len.end() ? 1 : len->second;
+      const int p = c.fb_cut ? (int)std::min<unsigned long long>(c.fb_cut, (unsigned long long)L) : L;
+      s->run_cap[start] = -p;
       PPVM_TRY(clear_err(s));
       s->n_ub = s->n_host;
       continue;

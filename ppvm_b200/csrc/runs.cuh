@@ -18,7 +18,8 @@
 // Kernels, in order: k_run_classify (group keys into a hash table, members counted; terms
 // outside every group compacted to the output with the truncation), k_run_order
 // (deterministic group numbering by first member, member offsets), k_run_scatter (member
-// lists), k_run_groups (butterfly + truncation + ordered write), k_run_commit (counts, op log).
+// lists), k_run_groups (butterfly + truncation + ordered write; its last block publishes the
+// counts and the op log).
 #pragma once
 
 #include "kernels.cuh"
@@ -126,27 +127,28 @@ k_run_classify(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, 
             if (wcap) keep = keep && (weight<W>(kx[it], kz[it]) <= maxw);
           }
         } else if (k > (unsigned)kRunMaxK) {
-          // the run's first g gates, g = the gate index of this term's (kRunMaxK+1)-th
-          // coordinate in gate order, hold at most kRunMaxK of its coordinates: the host
-          // cuts the run at the smallest such g over all terms (g >= kRunMaxK)
-          unsigned lo[kRunMaxK + 1];
-          unsigned nlo = 0;
+          // v is invariant through the run, so this term and all its descendants keep these
+          // k coordinates: the run from gate p on, p = 1 + the gate index of the term's
+          // (k - kRunMaxK)-th coordinate in gate order, holds at most kRunMaxK of them.  The
+          // host runs the gates before the largest such p one at a time and fuses the rest.
+          unsigned hi[kRunMaxK + 1];  // the kRunMaxK+1 largest gate indices, descending
+          unsigned nhi = 0;
 #pragma unroll
           for (int w = 0; w < W; ++w) {
             uint64_t m = M[w];
             while (m) {
               unsigned gi = s_gidx[w * 64 + (__ffsll((long long)m) - 1)];
               m &= m - 1;
-              if (nlo == kRunMaxK + 1 && gi >= lo[kRunMaxK]) continue;
-              unsigned r = nlo < kRunMaxK + 1 ? nlo++ : kRunMaxK;
-              while (r > 0 && lo[r - 1] > gi) {
-                lo[r] = lo[r - 1];
+              if (nhi == kRunMaxK + 1 && gi <= hi[kRunMaxK]) continue;
+              unsigned r = nhi < kRunMaxK + 1 ? nhi++ : kRunMaxK;
+              while (r > 0 && hi[r - 1] < gi) {
+                hi[r] = hi[r - 1];
                 --r;
               }
-              lo[r] = gi;
+              hi[r] = gi;
             }
           }
-          atomicMax(&ctrl->fb_cut, 65536ull - lo[kRunMaxK]);
+          atomicMax(&ctrl->fb_cut, (unsigned long long)hi[kRunMaxK] + 1ull);
           set_err(ctrl, kErrFallback, op);
           R.gslot[i] = kNone;
         } else {
@@ -345,6 +347,60 @@ __global__ void __launch_bounds__(256) k_run_scatter(Planes P, Ctrl* ctrl, const
   }
 }
 
+// Publishes the count after the run and fills the op log of its gates (and its TRUNCATE):
+// one warp of the last block of k_run_groups.  Gate j's live count is n0 plus the children
+// the gates before it created (an exclusive scan of the created counts, 8 gates per lane).
+__device__ __forceinline__ void run_commit(Ctrl* ctrl, RunScratch R, int op0, int L, int trunc_op, OpLog* log) {
+  const unsigned lane = threadIdx.x & 31;
+  if (ld_volatile_int(&ctrl->err)) {
+    if (lane < 4) ctrl->tickets[lane] = 0;
+    return;
+  }
+  constexpr int PER = kRunMaxGates / 32;
+  unsigned long long made[PER], tot = 0;
+#pragma unroll
+  for (int e = 0; e < PER; ++e) {
+    const int j = (int)lane * PER + e;
+    made[e] = j < L ? ld_volatile(&R.created[j]) : 0ull;
+    tot += made[e];
+  }
+  unsigned long long incl = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= (unsigned)o) incl += t;
+  }
+  const unsigned long long total = __shfl_sync(kFull, incl, 31);
+  const unsigned long long n0 = ld_volatile(&ctrl->n);
+  unsigned long long run = n0 + incl - tot;
+#pragma unroll
+  for (int e = 0; e < PER; ++e) {
+    const int j = (int)lane * PER + e;
+    if (j < L) {
+      log[op0 + j].n_in = run;
+      run += made[e];
+      log[op0 + j].n_new = made[e];
+      log[op0 + j].n_out = run;
+      log[op0 + j].n_s = 0;
+      R.created[j] = 0;  // clean for the next run
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs);
+    const unsigned long long nun = ld_volatile(&ctrl->n_s), cap_needed = ld_volatile(&ctrl->cap_needed);
+    for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
+    log[op0].n_s = ld_volatile(&ctrl->n_side);  // touched terms (profiling bytes)
+    if (L > 1) log[op0 + L - 1].n_s = (ngroups == 0) ? 0 : cap_needed - nun;  // group outputs
+    const unsigned long long out = (ngroups == 0) ? nun : cap_needed;
+    if (trunc_op >= 0) {
+      log[trunc_op].n_in = n0 + total;
+      log[trunc_op].n_out = out;
+    }
+    ctrl->n = out;
+  }
+}
+
 // One warp per group: butterfly over the group's coordinates, gates in run order.  Warps
 // are independent: each takes its next group by ticket, so groups of very different sizes do
 // not hold each other up at block barriers.  The group number is also the look-back tile,
@@ -352,7 +408,7 @@ __global__ void __launch_bounds__(256) k_run_scatter(Planes P, Ctrl* ctrl, const
 template <int W>
 __global__ void __launch_bounds__(kRunWarps * 32)
 k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, int trunc, double thr,
-             unsigned long long maxw, unsigned long long* ts, unsigned epoch, int op) {
+             unsigned long long maxw, unsigned long long* ts, unsigned epoch, int op, int trunc_op, OpLog* log) {
   pdl_wait();
   constexpr int SZ = 1 << kRunMaxK;
   __shared__ double s_coef[kRunWarps][SZ];
@@ -522,57 +578,7 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   __syncthreads();
   for (unsigned j = threadIdx.x; j < L; j += blockDim.x)
     if (s_created[j]) atomicAdd(&R.created[j], s_created[j]);
-}
-
-// Publishes the count after the run and fills the op log of its gates (and its TRUNCATE).
-// One block of kRunMaxGates threads: thread j logs gate j (an inclusive scan of the created
-// counts gives each gate's live count).
-static __global__ void __launch_bounds__(kRunMaxGates) k_run_commit(Ctrl* ctrl, RunScratch R, int op0, int L,
-                                                                    int trunc_op, OpLog* log) {
-  pdl_wait();
-  __shared__ unsigned long long s_w[kRunMaxGates / 32];
-  __shared__ int s_err;
-  if (threadIdx.x == 0) s_err = ctrl->err;
-  __syncthreads();
-  if (s_err) {
-    if (threadIdx.x < 4) ctrl->tickets[threadIdx.x] = 0;
-    return;
-  }
-  const unsigned long long n0 = ctrl->n, ngroups = ctrl->n_pairs;
-  const int j = threadIdx.x, lane = j & 31, warp = j >> 5;
-  const unsigned long long mine = j < L ? R.created[j] : 0ull;
-  unsigned long long incl = mine;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned long long t = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += t;
-  }
-  if (lane == 31) s_w[warp] = incl;
-  __syncthreads();
-  unsigned long long before = 0;
-  for (int w = 0; w < warp; ++w) before += s_w[w];
-  incl += before;
-  unsigned long long total = 0;
-  for (int w = 0; w < kRunMaxGates / 32; ++w) total += s_w[w];
-  if (j < L) {
-    log[op0 + j].n_in = n0 + incl - mine;
-    log[op0 + j].n_new = mine;
-    log[op0 + j].n_out = n0 + incl;
-    log[op0 + j].n_s = 0;
-    R.created[j] = 0;  // clean for the next run
-  }
-  __syncthreads();
-  if (j == 0) {
-    for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
-    log[op0].n_s = ctrl->n_side;  // touched terms (profiling bytes)
-    if (L > 1) log[op0 + L - 1].n_s = (ngroups == 0) ? 0 : ctrl->cap_needed - ctrl->n_s;  // group outputs
-    const unsigned long long out = (ngroups == 0) ? ctrl->n_s : ctrl->cap_needed;
-    if (trunc_op >= 0) {
-      log[trunc_op].n_in = n0 + total;
-      log[trunc_op].n_out = out;
-    }
-    ctrl->n = out;
-  }
+  if (last_block_done(&ctrl->done) && warp == 0) run_commit(ctrl, R, op, (int)L, trunc_op, log);
 }
 
 }  // namespace ppvm

@@ -151,12 +151,13 @@ __device__ __forceinline__ unsigned tab_map(const uint64_t* rows, const uint8_t*
 }
 
 // Maps every live term through the run; with trunc, drops what the strategy drops.  Survivors
-// go to O in input order; the count is left in ctrl->n_s for k_commit_tableau.
+// go to O in input order; the last block to finish publishes their count (and the log of the
+// fused TRUNCATE, trunc_op).
 template <int W, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_tableau(Planes P, Planes O, Ctrl* ctrl, TabParams tp, const uint64_t* __restrict__ g_rows,
           const uint8_t* __restrict__ g_ph, int trunc, double thr, unsigned long long maxw,
-          unsigned long long* ts, unsigned epoch, int op0, int nops, OpLog* log) {
+          unsigned long long* ts, unsigned epoch, int op0, int nops, int trunc_op, OpLog* log) {
   pdl_wait();
   extern __shared__ __align__(16) uint64_t s_rows[];  // nrows * 2W words, then nrows phase bytes
   __shared__ unsigned s_tile;
@@ -222,21 +223,18 @@ k_tableau(Planes P, Planes O, Ctrl* ctrl, TabParams tp, const uint64_t* __restri
     }
     if (tile == ntiles - 1 && threadIdx.x == 0) ctrl->n_s = excl + agg;
   }
-}
-
-// Publishes the count after a tableau pass (and fills the log of its fused TRUNCATE).
-static __global__ void k_commit_tableau(Ctrl* ctrl, int trunc_op, OpLog* log) {
-  pdl_wait();
-  for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
-  if (ctrl->err) return;
-  const unsigned long long n_in = ctrl->n, n_out = ctrl->n_s;
-  if (trunc_op >= 0) {
-    log[trunc_op].n_in = n_in;
-    log[trunc_op].n_s = n_out;
-    log[trunc_op].n_new = 0;
-    log[trunc_op].n_out = n_out;
+  if (last_block_done(&ctrl->done) && threadIdx.x == 0) {
+    for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
+    if (ld_volatile_int(&ctrl->err)) return;
+    const unsigned long long n_out = N == 0 ? 0ull : ld_volatile(&ctrl->n_s);
+    if (trunc_op >= 0) {
+      log[trunc_op].n_in = N;
+      log[trunc_op].n_s = n_out;
+      log[trunc_op].n_new = 0;
+      log[trunc_op].n_out = n_out;
+    }
+    ctrl->n = n_out;
   }
-  ctrl->n = n_out;
 }
 
 }  // namespace ppvm

@@ -202,9 +202,10 @@ def test_capacity_growth_replay():
 
 
 def test_wide_run_splits_until_it_fits():
-    # Z on qubits 0..11 meets a 40-gate RX run in qubit order: 12 > 10 coordinates, so the
-    # run is cut where that term's 11th coordinate comes (10 gates) and the rest fuses as a
-    # second run; the RZ and RX layers after it cut again on a larger sum
+    # Z on qubits 0..11 meets a 40-gate RX run in qubit order: 12 > 10 coordinates.  The
+    # group keeps them through the whole run, so after its 2nd coordinate (gate 1) at most 10
+    # remain: gates 0 and 1 replay one at a time and gates 2..39 fuse.  The RZ and RX layers
+    # after it meet wide groups again on a larger sum
     n = 40
     rng = np.random.default_rng(7)
     terms = {"Z" * 12 + "I" * (n - 12): 1.0}
@@ -217,6 +218,15 @@ def test_wide_run_splits_until_it_fits():
     ops += [G.r1(G.RZ, q, 0.3) for q in range(n)] + [G.truncate()]
     ops += [G.r1(G.RX, q, -0.2) for q in range(n)] + [G.truncate()]
     run_both(list(terms.items()), n, ops, thr=1e-6, check_every=n + 1, exact=False)
+
+
+def test_wide_run_fuses_its_tail():
+    # Z on qubits 20..31 meets a 32-gate RX run in qubit order: the first 22 gates (up to its
+    # 2nd coordinate) go one at a time and the last 10 fuse
+    n = 32
+    terms = [("I" * 20 + "Z" * 12, 1.0), ("X" + "I" * 30 + "Y", -0.5), ("IZ" + "I" * 30, 0.25)]
+    ops = [G.r1(G.RX, q, 0.35) for q in range(n)] + [G.truncate()]
+    run_both(terms, n, ops, thr=1e-7, exact=False)
 
 
 @pytest.mark.parametrize("exact", [True, False])
