@@ -32,6 +32,7 @@ struct ppvm_mlp {
   float* v = nullptr;
   float* grads = nullptr;
   float* loss = nullptr;    // [0] = sum of squared errors of the last pass
+  float* slabs = nullptr;   // [kMaxTrainBlocks][kSlab]: per-block gradient partials + loss
   MlpWeights* w = nullptr;  // packed device weights
   int step = 0;
   float* d_feats = nullptr;  // training / prediction inputs (grown on demand)
@@ -49,6 +50,8 @@ int mlp_device(const ppvm_mlp* m) { return m ? m->device : -1; }
 namespace {
 
 constexpr int kTrainWarps = 4;
+constexpr int kMaxTrainBlocks = 296;
+constexpr int kSlab = (kMlpParams + 1 + 3) & ~3;  // the parameters' gradients, then the block's loss
 
 ppvm_status mfail(ppvm_status s, const std::string& msg) {
   ppvm::set_last_error(msg);
@@ -89,21 +92,26 @@ __global__ void k_mlp_pack(const float* p, MlpWeights* w) {
   if (threadIdx.x == 0) w->b3 = p[kOffB3];
 }
 
-// Adam on the flat parameter vector, one thread per parameter: the update, the gradient
-// cleared, and the parameter's own packed copies written (W1's zero padding is set once by
-// k_mlp_pack), so no thread waits for another.
-__global__ void __launch_bounds__(256) k_mlp_adam(float* p, float* m, float* v, float* g, MlpWeights* w, float lr_t,
-                                                  float b1, float b2, float eps) {
+// Adam on the flat parameter vector, one thread per parameter: the minibatch gradient (the
+// training blocks' slabs summed in block order), the update, and the parameter's own packed
+// copies written (W1's zero padding is set once by k_mlp_pack), so no thread waits for another.
+__global__ void __launch_bounds__(256) k_mlp_adam(float* p, float* m, float* v, const float* slabs, int nslabs,
+                                                  float* loss, MlpWeights* w, float lr_t, float b1, float b2,
+                                                  float eps) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= kMlpParams) return;
-  const float gi = g[i];
+  if (i > kMlpParams) return;
+  float gi = 0.0f;  // the minibatch gradient: slabs summed in block order
+  for (int b = 0; b < nslabs; ++b) gi += slabs[(size_t)b * kSlab + i];
+  if (i == kMlpParams) {  // the loss slot
+    *loss += gi;
+    return;
+  }
   const float mi = b1 * m[i] + (1.0f - b1) * gi;
   const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
   m[i] = mi;
   v[i] = vi;
   const float pi = p[i] - lr_t * mi / (sqrtf(vi) + eps);
   p[i] = pi;
-  g[i] = 0.0f;
   if (i < kOffB1) {
     const int n = (i - kOffW1) / kMlpIn, k = (i - kOffW1) % kMlpIn;
     w->w1[n * kMlpK1 + k] = __float2bfloat16_rn(pi);
@@ -154,31 +162,36 @@ __device__ __forceinline__ void add_cols(float* sG, int off, int j, float lo, fl
   hi += __shfl_xor_sync(0xffffffffu, hi, 8);
   hi += __shfl_xor_sync(0xffffffffu, hi, 16);
   const int lane = threadIdx.x & 31;
-  if (lane < 4) {
-    atomicAdd(&sG[off + 8 * j + 2 * lane], lo);
-    atomicAdd(&sG[off + 8 * j + 2 * lane + 1], hi);
+  if (lane < 4) {  // the warp's own gradient copy: each entry always written by the same lane
+    sG[off + 8 * j + 2 * lane] += lo;
+    sG[off + 8 * j + 2 * lane + 1] += hi;
   }
 }
 
 // Forward + backward over samples order[start .. start+count) of (feats, targets): squared
-// error loss scaled by inv_n; gradients added to `grads` (flat, FP32), the loss sum to *loss.
+// error loss scaled by inv_n.  Deterministic: every warp accumulates into its own gradient copy
+// (each entry always updated by the same lane), the block sums its warps' copies in a fixed
+// order into its slab (slabs[blockIdx.x]: gradients, then the loss), and the consumer sums the
+// slabs in block order.
 __global__ void __launch_bounds__(kTrainWarps * 32)
 k_mlp_train(const MlpWeights* Wg, const float* feats, const float* targets, const uint32_t* order,
-            unsigned long long start, unsigned long long count, float inv_n, float* grads, float* loss) {
+            unsigned long long start, unsigned long long count, float inv_n, float* slabs) {
   extern __shared__ __align__(16) unsigned char smem[];
   MlpWeights& W = *reinterpret_cast<MlpWeights*>(smem);
-  float* sG = reinterpret_cast<float*>(smem + sizeof(MlpWeights));
-  __nv_bfloat16* sX0 = reinterpret_cast<__nv_bfloat16*>(sG + ((kMlpParams + 3) & ~3));
+  float* sG0 = reinterpret_cast<float*>(smem + sizeof(MlpWeights));  // kTrainWarps copies of kSlab
+  __nv_bfloat16* sX0 = reinterpret_cast<__nv_bfloat16*>(sG0 + kTrainWarps * kSlab);
+  __shared__ float s_loss[kTrainWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   __nv_bfloat16* sX = sX0 + warp * (16 * kMlpK1 + 2 * 16 * kMlpH);
+  float* sG = sG0 + warp * kSlab;
   __nv_bfloat16* sD = sX + 16 * kMlpK1;  // [16][64]: dZ2, later dZ1
   __nv_bfloat16* sH = sD + 16 * kMlpH;   // [16][64]: H1
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(Wg);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&W);
     for (int i = threadIdx.x; i < (int)(sizeof(MlpWeights) / 4); i += blockDim.x) dst[i] = src[i];
-    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) sG[i] = 0.0f;
+    for (int i = threadIdx.x; i < kTrainWarps * kSlab; i += blockDim.x) sG0[i] = 0.0f;
   }
   __syncthreads();
   float lsum = 0.0f;
@@ -220,7 +233,7 @@ k_mlp_train(const MlpWeights* Wg, const float* feats, const float* targets, cons
       float s = (t == 0) ? dy[0] + dy[1] : 0.0f;
 #pragma unroll
       for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) atomicAdd(&sG[kOffB3], s);
+      if (lane == 0) sG[kOffB3] += s;
     }
     // stage dZ2 and H1 (BF16, row-major [16][64]) for the weight gradient of layer 2
 #pragma unroll
@@ -253,10 +266,10 @@ k_mlp_train(const MlpWeights* Wg, const float* feats, const float* targets, cons
         float acc[4] = {0.f, 0.f, 0.f, 0.f};
         mma_bf16(acc, a, b0, b1);
         const int col = 8 * j + 2 * t;
-        atomicAdd(&sG[kOffW2 + n0 * kMlpH + col], acc[0]);
-        atomicAdd(&sG[kOffW2 + n0 * kMlpH + col + 1], acc[1]);
-        atomicAdd(&sG[kOffW2 + (n0 + 8) * kMlpH + col], acc[2]);
-        atomicAdd(&sG[kOffW2 + (n0 + 8) * kMlpH + col + 1], acc[3]);
+        sG[kOffW2 + n0 * kMlpH + col] += acc[0];
+        sG[kOffW2 + n0 * kMlpH + col + 1] += acc[1];
+        sG[kOffW2 + (n0 + 8) * kMlpH + col] += acc[2];
+        sG[kOffW2 + (n0 + 8) * kMlpH + col + 1] += acc[3];
       }
     }
     // dH1 = dZ2 W2 (A from the dZ2 fragments, B = W2T), dZ1 = dH1 * gelu'(Z1)
@@ -305,19 +318,40 @@ k_mlp_train(const MlpWeights* Wg, const float* feats, const float* targets, cons
       const uint32_t b1 = pack2(sX[(2 * t + 8) * kMlpK1 + g], sX[(2 * t + 9) * kMlpK1 + g]);
       float acc[4] = {0.f, 0.f, 0.f, 0.f};
       mma_bf16(acc, a, b0, b1);
-      atomicAdd(&sG[kOffW1 + n0 * kMlpIn + 2 * t], acc[0]);
-      atomicAdd(&sG[kOffW1 + n0 * kMlpIn + 2 * t + 1], acc[1]);
-      atomicAdd(&sG[kOffW1 + (n0 + 8) * kMlpIn + 2 * t], acc[2]);
-      atomicAdd(&sG[kOffW1 + (n0 + 8) * kMlpIn + 2 * t + 1], acc[3]);
+      sG[kOffW1 + n0 * kMlpIn + 2 * t] += acc[0];
+      sG[kOffW1 + n0 * kMlpIn + 2 * t + 1] += acc[1];
+      sG[kOffW1 + (n0 + 8) * kMlpIn + 2 * t] += acc[2];
+      sG[kOffW1 + (n0 + 8) * kMlpIn + 2 * t + 1] += acc[3];
     }
     __syncwarp();  // sX, sD and sH are rewritten by the next tile
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x)
-    if (sG[i] != 0.0f) atomicAdd(&grads[i], sG[i]);
 #pragma unroll
   for (int o = 16; o; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-  if (lane == 0 && lsum != 0.0f) atomicAdd(loss, lsum);
+  if (lane == 0) s_loss[warp] = lsum;
+  __syncthreads();
+  float* slab = slabs + (size_t)blockIdx.x * kSlab;
+  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
+    float v = sG0[i];
+#pragma unroll
+    for (int w = 1; w < kTrainWarps; ++w) v += sG0[w * kSlab + i];
+    slab[i] = v;
+  }
+  if (threadIdx.x == 0) {
+    float l = s_loss[0];
+    for (int w = 1; w < kTrainWarps; ++w) l += s_loss[w];
+    slab[kMlpParams] = l;
+  }
+}
+
+// Sums the slabs of k_mlp_train's blocks in block order: the gradient (one thread per
+// parameter), and the loss into *loss (thread kMlpParams).
+__global__ void __launch_bounds__(256) k_mlp_reduce(const float* slabs, int nslabs, float* grads, float* loss) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > kMlpParams) return;
+  float v = 0.0f;
+  for (int b = 0; b < nslabs; ++b) v += slabs[(size_t)b * kSlab + i];
+  if (i < kMlpParams) grads[i] = v;
+  else *loss += v;
 }
 
 // Scores of n feature rows (one warp per 16 rows).
@@ -347,7 +381,7 @@ __global__ void __launch_bounds__(128) k_mlp_predict(const MlpWeights* Wg, const
 }
 
 size_t train_smem() {
-  return sizeof(MlpWeights) + sizeof(float) * ((kMlpParams + 3) & ~3) +
+  return sizeof(MlpWeights) + sizeof(float) * kTrainWarps * kSlab +
          sizeof(__nv_bfloat16) * kTrainWarps * (16 * kMlpK1 + 2 * 16 * kMlpH);
 }
 
@@ -370,19 +404,22 @@ ppvm_status ensure_data(ppvm_mlp* m, size_t n) {
   return PPVM_OK;
 }
 
-ppvm_status launch_train(ppvm_mlp* m, bool use_order, unsigned long long start, unsigned long long count, float inv_n) {
+// Forward + backward of one minibatch into the slabs; *nslabs = the number of slabs written.
+ppvm_status launch_train(ppvm_mlp* m, bool use_order, unsigned long long start, unsigned long long count, float inv_n,
+                         int* nslabs) {
   static unsigned long long attr = 0;
   if (!((attr >> m->device) & 1ull)) {
     MCUDA(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem()));
     attr |= 1ull << m->device;
   }
   const unsigned long long tiles = (count + 15) / 16;
-  const unsigned grid = (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>(
-                                                                      (tiles + kTrainWarps - 1) / kTrainWarps, 296));
+  const unsigned grid = (unsigned)std::max<unsigned long long>(
+      1, std::min<unsigned long long>((tiles + kTrainWarps - 1) / kTrainWarps, kMaxTrainBlocks));
   k_mlp_train<<<grid, kTrainWarps * 32, train_smem(), m->stream>>>(m->w, m->d_feats, m->d_tgt,
                                                                    use_order ? m->d_order : nullptr, start, count,
-                                                                   inv_n, m->grads, m->loss);
+                                                                   inv_n, m->slabs);
   MCUDA(cudaGetLastError());
+  *nslabs = (int)grid;
   return PPVM_OK;
 }
 
@@ -407,6 +444,7 @@ ppvm_status ppvm_mlp_destroy(ppvm_mlp* m) {
   cudaFree(m->v);
   cudaFree(m->grads);
   cudaFree(m->loss);
+  cudaFree(m->slabs);
   cudaFree(m->w);
   cudaFree(m->d_feats);
   cudaFree(m->d_tgt);
@@ -423,7 +461,6 @@ ppvm_status ppvm_mlp_set_params(ppvm_mlp* m, const float* params, size_t n) {
   MCUDA(cudaMemcpyAsync(m->params, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, m->stream));
   MCUDA(cudaMemsetAsync(m->m, 0, sizeof(float) * kMlpParams, m->stream));
   MCUDA(cudaMemsetAsync(m->v, 0, sizeof(float) * kMlpParams, m->stream));
-  MCUDA(cudaMemsetAsync(m->grads, 0, sizeof(float) * kMlpParams, m->stream));
   k_mlp_pack<<<1, 256, 0, m->stream>>>(m->params, m->w);
   MCUDA(cudaGetLastError());
   MCUDA(cudaStreamSynchronize(m->stream));
@@ -454,7 +491,8 @@ ppvm_status ppvm_mlp_create(ppvm_mlp** out, uint64_t seed, int device) {
       cudaMalloc(&m->m, sizeof(float) * kMlpParams) != cudaSuccess ||
       cudaMalloc(&m->v, sizeof(float) * kMlpParams) != cudaSuccess ||
       cudaMalloc(&m->grads, sizeof(float) * kMlpParams) != cudaSuccess ||
-      cudaMalloc(&m->loss, sizeof(float)) != cudaSuccess || cudaMalloc(&m->w, sizeof(MlpWeights)) != cudaSuccess) {
+      cudaMalloc(&m->loss, sizeof(float)) != cudaSuccess || cudaMalloc(&m->w, sizeof(MlpWeights)) != cudaSuccess ||
+      cudaMalloc(&m->slabs, sizeof(float) * kSlab * kMaxTrainBlocks) != cudaSuccess) {
     ppvm_mlp_destroy(m);
     return mfail(PPVM_ECAPACITY, "device allocation failed");
   }
@@ -480,13 +518,14 @@ ppvm_status ppvm_mlp_grad(ppvm_mlp* m, const float* feats, const float* targets,
   MTRY(ensure_data(m, n));
   MCUDA(cudaMemcpyAsync(m->d_feats, feats, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice, m->stream));
   MCUDA(cudaMemcpyAsync(m->d_tgt, targets, sizeof(float) * n, cudaMemcpyHostToDevice, m->stream));
-  MCUDA(cudaMemsetAsync(m->grads, 0, sizeof(float) * kMlpParams, m->stream));
   MCUDA(cudaMemsetAsync(m->loss, 0, sizeof(float), m->stream));
-  MTRY(launch_train(m, false, 0, n, 1.0f / (float)n));
+  int nslabs = 0;
+  MTRY(launch_train(m, false, 0, n, 1.0f / (float)n, &nslabs));
+  k_mlp_reduce<<<(kMlpParams + 1 + 255) / 256, 256, 0, m->stream>>>(m->slabs, nslabs, m->grads, m->loss);
+  MCUDA(cudaGetLastError());
   MCUDA(cudaMemcpyAsync(grads, m->grads, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, m->stream));
   float ls = 0.f;
   MCUDA(cudaMemcpyAsync(&ls, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
-  MCUDA(cudaMemsetAsync(m->grads, 0, sizeof(float) * kMlpParams, m->stream));
   MCUDA(cudaStreamSynchronize(m->stream));
   if (loss) *loss = ls / (float)n;
   return PPVM_OK;
@@ -512,11 +551,12 @@ ppvm_status ppvm_mlp_train(ppvm_mlp* m, const float* feats, const float* targets
     MCUDA(cudaMemsetAsync(m->loss, 0, sizeof(float), m->stream));
     for (size_t st = 0; st < n; st += (size_t)batch) {
       const size_t cnt = std::min<size_t>((size_t)batch, n - st);
-      MTRY(launch_train(m, true, st, cnt, 1.0f / (float)cnt));
+      int nslabs = 0;
+      MTRY(launch_train(m, true, st, cnt, 1.0f / (float)cnt, &nslabs));
       ++m->step;
       const float lr_t = lr * std::sqrt(1.0f - std::pow(b2, (float)m->step)) / (1.0f - std::pow(b1, (float)m->step));
-      k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, m->stream>>>(m->params, m->m, m->v, m->grads, m->w, lr_t,
-                                                                   b1, b2, eps);
+      k_mlp_adam<<<(kMlpParams + 1 + 255) / 256, 256, 0, m->stream>>>(m->params, m->m, m->v, m->slabs, nslabs,
+                                                                       m->loss, m->w, lr_t, b1, b2, eps);
       MCUDA(cudaGetLastError());
     }
     MCUDA(cudaMemcpyAsync(&ls, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));

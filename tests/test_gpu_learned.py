@@ -60,6 +60,22 @@ def test_training_fits_a_smooth_target():
     assert after < 0.05 * before and after < 0.02, (before, after)
 
 
+def test_training_is_deterministic():
+    """Same data, seed and start: bit-identical gradients and trained parameters (no float
+    atomics: per-warp copies, per-block slabs, fixed-order sums)."""
+    rng = np.random.default_rng(6)
+    X = rng.normal(0, 1, (3000, 8)).astype(np.float32)
+    t = rng.normal(0, 1, 3000).astype(np.float32)
+    runs = []
+    for _ in range(2):
+        net, _ = rand_net(5)
+        g, loss = net.grad(X, t)
+        net.train(X, t, epochs=3, batch=256, lr=1e-3, seed=9)
+        runs.append((g, loss, net.params))
+    assert np.array_equal(runs[0][0], runs[1][0]) and runs[0][1] == runs[1][1]
+    assert np.array_equal(runs[0][2], runs[1][2])
+
+
 def test_adam_step_and_repacked_weights():
     """One full-batch step: Adam's first update is -lr * sign(g) (bias-corrected moments), and
     the packed tensor-core weights follow the updated FP32 parameters."""
