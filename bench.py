@@ -202,6 +202,24 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def over_ranks(values, device, op: str = "max") -> list[float]:
+    """The elementwise max (or sum) of ``values`` over all ranks; the values themselves on one
+    rank.  ``device`` is the rank's CUDA device under NCCL, the CPU under gloo."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(v) for v in t.cpu()]
+
+
+def batched_shard_seed(rank: int) -> int:
+    """Rank r of the batched workload propagates the 256 instances of seed 1 + r: the ranks'
+    shards are independent instances, and rank 0's shard is the single-GPU batch."""
+    return 1 + rank
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -313,11 +331,8 @@ def run_gpu(args):
         del s
     e2e_s = sum(e2e_ms) / 1e3
 
-    # ---- max over ranks ----------------------------------------------------------------------
-    t_dev = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
-    dev_s, e2e_s = float(t_dev[0]), float(t_dev[1])
+    # ---- max over ranks (each rank propagates a replica of the sum) ----------------------------
+    dev_s, e2e_s = over_ranks([dev_s, e2e_s], dev, "max")
     total_updates = updates * args.steps * world
     value = total_updates / dev_s
     e2e_value = total_updates / e2e_s
@@ -375,7 +390,9 @@ BATCH_CPU_SAMPLE = 64  # instances of the batched workload timed on the host CPU
 def batched_config(n_inst, world, extra=None):
     d = {"workload": f"batched_tfim: {n_inst} independent 1D TFIM instances (seed 1), n ~ U[16,128], "
                      "steps ~ U[5,30], h ~ U[0.5,1.5], J=1, dt=0.05, obs Z(n/2), thr 1e-5",
-         "instances": n_inst, "parallelism": f"replicas x{world}" if world > 1 else "one batch"}
+         "instances": n_inst,
+         "parallelism": (f"{world} shards of {n_inst} instances: rank r holds seed 1 + r" if world > 1
+                         else "one batch")}
     if extra:
         d.update(extra)
     return d
@@ -434,7 +451,7 @@ def run_batched(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    wls = C.batched_tfim()
+    wls = C.batched_tfim(seed=batched_shard_seed(rank))
     b = PauliSumBatch.from_workloads(wls, device=local)
     b.set_stream(stream.cuda_stream)
     clk = ClockSampler(local)  # started before the warm-up: its first query is not in the timed region
@@ -490,15 +507,15 @@ def run_batched(args):
         seq_s = time.perf_counter() - t
         seq = {"value": tgu / seq_s, "unit": METRIC, "ms_to_all_O": 1e3 * seq_s,
                "what": "the 256 instances one after another through the plain single-sum engine (PauliSum)"}
-    t_dev = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
-    dev_s, e2e_s = float(t_dev[0]), float(t_dev[1])
+    # each rank propagates its own shard of instances: the job's updates are the sum over ranks,
+    # its time the max
+    dev_s, e2e_s = over_ranks([dev_s, e2e_s], dev, "max")
+    tgu_job = int(over_ranks([tgu], dev, "sum")[0])
     if rank == 0:
         peak_gbs, peak_kind = measured_peak()
         # algorithmic bytes: every term-gate update reads the X and Z word holding the gate's qubit
         achieved = 16.0 * tgu * args.steps / dev_s / 1e9
-        line = {"metric": METRIC, "value": tgu * args.steps * world / dev_s, "unit": METRIC, "n_gpus": world,
+        line = {"metric": METRIC, "value": tgu_job * args.steps / dev_s, "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (generated circuits)",
@@ -506,7 +523,7 @@ def run_batched(args):
                                                            "term_gate_updates_per_step": tgu,
                                                            "launch_config": tune,
                                                            "max_live_terms": int(max(b.len_of(j) for j in range(len(wls))))}),
-                "e2e": {"value": tgu * args.steps * world / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "e2e": {"value": tgu_job * args.steps / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_s / args.steps},
                 "time_to_all_O_ms": 1e3 * dev_s / args.steps,
                 "sequential_plain_gpu": seq,
