@@ -1072,7 +1072,11 @@ ppvm_status ppvm_batch_get_config(const ppvm_batch* b, int* block, int* items, i
 
 ppvm_status ppvm_batch_run(ppvm_batch* b) {
   if (!b) return bfail(PPVM_EINVAL, "null batch");
-  return run_all(b, true, false);
+  // Layer graphs pay off from the second run of an unchanged batch on.  A batch's first run
+  // (and the first after new ops or a new layout) launches the layers directly, which saves
+  // capturing and instantiating one graph per layer for a batch that runs once.
+  const bool reuse = b->ran && !b->ops_dirty && !b->layout_dirty;
+  return run_all(b, reuse, false);
 }
 
 ppvm_status ppvm_batch_run_persistent(ppvm_batch* b) {

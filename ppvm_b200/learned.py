@@ -156,7 +156,7 @@ def run_with_budget(wl, budget: int | None, net=None, lattice: int = 0, device: 
 
 
 def compare_budgets(L: int = 10, layers: int = 4, seed: int = 2,
-                    budgets=(500, 1000, 2000, 4000, 8000, 1_000_000, 4_000_000),
+                    budgets=(500, 700, 1000, 1400, 2000, 2800, 4000, 5600, 8000, 1_000_000, 4_000_000),
                     train_L: int = 6, train_layers: int = 4, train_seeds=(11, 12, 13, 14, 15, 16, 17, 18),
                     per_layer: int = 2048, epochs: int = 300, label_thr: float = 1e-5, device: int = 0,
                     tol: float = 1e-3, log=None):
