@@ -220,6 +220,14 @@ def batched_shard_seed(rank: int) -> int:
     return 1 + rank
 
 
+# DRAM bytes (read + write) of one launch of the kernel, from one ncu capture of this workload
+# (profiles/k_run_groups_kicked_ising_12x12.md and k_tableau_kicked_ising_12x12.md: a layer
+# with about 2e5 terms entering).  Far below the algorithmic bytes: the sum stays in L2.
+CAPTURED_TRAFFIC = {"run_groups": 379648 + 14336, "tableau": 3266560 + 256}
+TRAFFIC_SOURCE = ("ncu --set full capture of one launch of each kernel (the first two matches after skipping "
+                  "76, command in profiles/), dram__bytes_read.sum + dram__bytes_write.sum")
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -347,7 +355,9 @@ def run_gpu(args):
             achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9
             roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
                     "frac": achieved / peak_gbs, "peak_kind": peak_kind,
-                    "traffic": None, "bytes_per_launch": d["bytes"] / d["launches"],
+                    "traffic": CAPTURED_TRAFFIC.get(dom),
+                    "traffic_source": TRAFFIC_SOURCE if dom in CAPTURED_TRAFFIC else None,
+                    "bytes_per_launch": d["bytes"] / d["launches"],
                     "avg_launch_us": 1e3 * d["ms"] / d["launches"],
                     "share_of_device_time": d["ms"] / (1e3 * prof_s) if prof_s else None,
                     "timing": "per-launch CUDA events on the sum's stream, in a second timed pass of the same steps "
