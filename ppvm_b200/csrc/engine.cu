@@ -86,12 +86,11 @@ struct ProfLaunch {
 
 enum Family {
   F_SCAN = 0, F_PAIR, F_APPLY, F_COMMIT, F_CLIFF, F_TRUNC, F_READ,
-  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_UNTOUCHED, F_RUN_GROUPS, F_RUN_COMMIT, F_TABLEAU, F_COUNT
+  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_GROUPS, F_TABLEAU, F_COUNT
 };
 const char* kFamilyNames[F_COUNT] = {"rot_scan", "rot_pair", "rot_apply", "rot_commit",
                                      "clifford", "truncate", "readout",
-                                     "run_classify", "run_order", "run_scatter", "run_untouched",
-                                     "run_groups", "run_commit", "tableau"};
+                                     "run_classify", "run_order", "run_scatter", "run_groups", "tableau"};
 
 // One pinned host chunk and its device twin: per-call uploads (op descriptors, run
 // descriptors, tableaux) are packed here and copied with truly asynchronous copies.
@@ -799,8 +798,9 @@ struct K {
     const void* d_rd_v = nullptr;
     PPVM_TRY(stage_put(s, &rd, sizeof(RunDesc), &d_rd_v));
     const RunDesc* d_rd = static_cast<const RunDesc*>(d_rd_v);
-    // grp_min, grp_cnt and created are clean here: k_run_scatter and k_run_commit reset what a
-    // run used, grow() clears them on allocation and run_list() after a device error
+    // grp_min, grp_cnt and created are clean here: k_run_scatter and the last block of
+    // k_run_groups reset what a run used, grow() clears them on allocation and run_list()
+    // after a device error
     const int trunc = trunc_op >= 0 ? 1 : 0;
     {
       ProfScope ps(s, F_RUN_CLASSIFY, op0, L);
