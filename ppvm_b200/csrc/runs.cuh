@@ -200,6 +200,10 @@ k_run_classify(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, 
 }
 
 // Numbers the groups by their smallest member (index order) and lays out member lists.
+// While the sum holds fewer than 2^21 terms (every block reads the same N), both running
+// counts travel in one look-back value, groups in the low 21 bits and members in the next 21:
+// one chain per tile instead of two.
+constexpr int kOrderPackBits = 21;
 template <int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long long* ts_b, unsigned ep_a,
@@ -273,8 +277,16 @@ k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long lo
     }
     __syncthreads();
     const unsigned long long agg_cnt = s_cnt[ITEMS * NW];
-    const unsigned long long excl = lookback(ts_a, tile, agg, ep_a, ctrl, op, &s_slot);
-    const unsigned long long excl_cnt = lookback(ts_b, tile, agg_cnt, ep_b, ctrl, op, &s_slot);
+    unsigned long long excl, excl_cnt;
+    if (N < (1ull << kOrderPackBits)) {
+      const unsigned long long both =
+          lookback(ts_a, tile, (unsigned long long)agg | (agg_cnt << kOrderPackBits), ep_a, ctrl, op, &s_slot);
+      excl = both & ((1ull << kOrderPackBits) - 1);
+      excl_cnt = both >> kOrderPackBits;
+    } else {
+      excl = lookback(ts_a, tile, agg, ep_a, ctrl, op, &s_slot);
+      excl_cnt = lookback(ts_b, tile, agg_cnt, ep_b, ctrl, op, &s_slot);
+    }
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k) {
       if ((ballots[k] >> lane) & 1u) {
