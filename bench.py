@@ -182,7 +182,11 @@ def run_reference(args):
 
 # ---------------------------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region, every 20 ms, through
+    NVML in this process (the library nvidia-smi reads them with): the SM clock, its maximum
+    and the clock-event reason bits, nothing else.  NVML is initialised before the warm-up.
+    Spawning nvidia-smi during the timed region stalled the GPU for milliseconds; an NVML
+    clock read does not.  Without NVML, one nvidia-smi process looping every 100 ms (-lms)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -192,21 +196,49 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self.times = []
+        self._p = None
+        self._nvml = None
         self._stop = threading.Event()
+        self._first = threading.Event()
         self._t = threading.Thread(target=self._loop, daemon=True)
 
+    def _nvml_handle(self):
+        import pynvml as nv
+
+        nv.nvmlInit()
+        try:  # the CUDA device's own GPU: NVML may number GPUs differently from CUDA
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nv, nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv, nv.nvmlDeviceGetHandleByIndex(self.index)
+
     def _loop(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
+        if self._nvml is not None:
+            nv, h = self._nvml
+            bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            while not self._stop.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    flags = ["Active" if rs & b else "Not Active" for b in bits]
+                    self.rows.append([str(self.index), str(sm), str(mx), "", hex(rs)] + flags)
                     self.times.append(time.perf_counter())
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+                except Exception:
+                    pass
+                self._first.set()
+                self._stop.wait(0.02)
+            return
+        for line in self._p.stdout:
+            line = line.strip()
+            if line:
+                self.rows.append([c.strip() for c in line.split(",")])
+                self.times.append(time.perf_counter())
+                self._first.set()
 
     def window(self, t0: float, t1: float) -> None:
         """Keeps the samples taken in [t0, t1] (or the one nearest to it if none was)."""
@@ -216,12 +248,31 @@ class ClockSampler:
         self.rows = [self.rows[i] for i in keep]
 
     def __enter__(self):
+        try:
+            self._nvml = self._nvml_handle()
+        except Exception:
+            self._nvml = None
+            try:
+                self._p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                            "--format=csv,noheader,nounits", "-lms", "100"],
+                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            except OSError:
+                return self  # neither NVML nor nvidia-smi: summary() reports the clocks as unavailable
         self._t.start()
+        self._first.wait(timeout=10)  # the first query, and its stall, before anything is timed
         return self
 
     def __exit__(self, *a):
         self._stop.set()
-        self._t.join(timeout=10)
+        if self._nvml is not None:
+            self._t.join(timeout=10)
+        if self._p is not None:
+            self._p.terminate()  # the process this sampler started
+            try:
+                self._p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._p.kill()
+            self._t.join(timeout=10)
 
     def summary(self):
         if not self.rows:
@@ -311,6 +362,14 @@ def run_gpu(args):
 
     # ---- device-resident timing: inputs already in HBM (sums created up front) -----------
     gate_list = ops_array(wl.ops)  # the circuit, packed once as ppvm_op records
+    # warm-up, continued: a sum's handle sizes its op log and upload arena on its first run
+    # (allocations that synchronise), and destroyed sums leave their handles to the library's
+    # cache.  So every handle the timed steps will use runs the circuit once here.
+    warm = [make(cap) for _ in range(args.steps)]
+    for s in warm:
+        s.run(gate_list)
+        s.overlap_with_zero()
+    del warm, s
 
     def timed_pass(per_launch_events: bool):
         sums = [make(cap) for _ in range(args.steps)]

@@ -956,8 +956,10 @@ ppvm_status ppvm_batch_set_ops(ppvm_batch* b, size_t inst, const ppvm_op* ops, s
   const uint32_t n = b->nq[inst];
   const double half_pi = 1.5707963267948966;
   std::vector<BOp> out;
+  out.reserve(n_ops);
   std::vector<uint32_t> le;
   int truncs = 0;
+  SinCosMemo trig;
   for (size_t i = 0; i < n_ops; ++i) {
     const ppvm_op& op = ops[i];
     if (op.flags != 0 || op.code >= PPVM_OP_COUNT_) return bfail(PPVM_EINVAL, "bad op code or flags");
@@ -992,8 +994,7 @@ ppvm_status ppvm_batch_set_ops(ppvm_batch* b, size_t inst, const ppvm_op* ops, s
         d.f0 = op.theta > 0 ? 1.0 : -1.0;
       } else {
         bo.kind = B_ROT;
-        bo.sn = std::sin(op.theta);
-        bo.cs = std::cos(op.theta);
+        trig.get(op.theta, bo.sn, bo.cs);
       }
     } else {
       bo.kind = B_LOCAL;

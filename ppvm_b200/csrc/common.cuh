@@ -4,10 +4,31 @@
 // term i lives at x[w * cap + i], Z plane likewise, coefficient at c[i].  W = ceil(n/64).
 #pragma once
 
+#include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 namespace ppvm {
+
+// Host: sin and cos of a gate angle, recomputed only when the angle's bit pattern changes
+// (gate lists repeat a few angles many times).  The values are the libm results either way;
+// comparing bits, not values, keeps -0.0 and +0.0 apart, as their sines differ in sign.
+struct SinCosMemo {
+  uint64_t bits = 0x7FF8DEADBEEF0001ull;  // a NaN pattern no caller passes
+  double sn = 0.0, cs = 0.0;
+  void get(double theta, double& s, double& c) {
+    uint64_t b;
+    std::memcpy(&b, &theta, sizeof(b));
+    if (b != bits) {
+      bits = b;
+      sn = std::sin(theta);
+      cs = std::cos(theta);
+    }
+    s = sn;
+    c = cs;
+  }
+};
 
 constexpr int kMaxW = 8;  // up to 512 qubits
 constexpr unsigned kFull = 0xffffffffu;

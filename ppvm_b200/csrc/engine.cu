@@ -988,6 +988,7 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
                     const std::vector<Gen>& gens, std::vector<int>& test_words) {
   std::vector<DevOp> run;  // pending local ops (Cliffords, Clifford-angle rotations, noise)
   int run_start = -1;
+  SinCosMemo trig;          // the fused runs' gate angles
   size_t per_gate_end = 0;  // ops before this index take the per-gate path (a wide run)
   s->d_perr2 = nullptr;
   if (!s->perr2_host.empty()) {
@@ -1084,8 +1085,7 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
         if ((rd.Q[o.q0 >> 6] >> (o.q0 & 63)) & 1ull) break;  // qubit repeats: end the run
         rd.Q[o.q0 >> 6] |= 1ull << (o.q0 & 63);
         rd.q[rd.L] = o.q0;
-        rd.sn[rd.L] = std::sin(o.theta);
-        rd.cs[rd.L] = std::cos(o.theta);
+        trig.get(o.theta, rd.sn[rd.L], rd.cs[rd.L]);
         ++rd.L;
         ++j;
       }
