@@ -236,9 +236,12 @@ k_run_order(Ctrl* ctrl, RunScratch R, unsigned long long* ts_a, unsigned long lo
       cnts[k] = 0;
       if (i < N) {
         const uint32_t s = R.gslot[i];
-        if (s != kNone && R.grp_min[s] == (uint32_t)i) {
-          rep = true;
-          cnts[k] = R.grp_cnt[s];
+        if (s != kNone) {
+          const uint32_t first = R.grp_min[s], cnt = R.grp_cnt[s];  // both loads in flight at once
+          if (first == (uint32_t)i) {
+            rep = true;
+            cnts[k] = cnt;
+          }
         }
       }
       ballots[k] = __ballot_sync(kFull, rep);
@@ -328,10 +331,11 @@ __global__ void __launch_bounds__(256) k_run_scatter(Planes P, Ctrl* ctrl, const
        i += (unsigned long long)gridDim.x * blockDim.x) {
     const uint32_t s = R.gslot[i];
     if (s == kNone) continue;
+    uint64_t x[W], z[W], v[W], f[W];
+    load_key<W>(P, i, x, z);  // the term's own data: in flight with the group lookups below
+    const double coef = P.c[i];
     const uint32_t o = R.grp_ord[s];
     const uint32_t pos = R.g_start[o] + atomicAdd(&R.g_fill[o], 1u);
-    uint64_t x[W], z[W], v[W], f[W];
-    load_key<W>(P, i, x, z);
     split_planes<W>(cls, x, z, v, f);
     unsigned c = 0, t = 0;
 #pragma unroll
@@ -345,7 +349,7 @@ __global__ void __launch_bounds__(256) k_run_scatter(Planes P, Ctrl* ctrl, const
       }
     }
     R.mcoord[pos] = c;
-    R.mcoef[pos] = P.c[i];
+    R.mcoef[pos] = coef;
     if (R.g_rep[o] == (uint32_t)i) {
       uint64_t* gk = R.gkey + (unsigned long long)o * 2 * W;
 #pragma unroll
