@@ -12,8 +12,9 @@ truncation and weight cap 10, FP64 coefficients, synthetic inputs (the circuit i
 
 Arms:
   default           the CUDA engine through its C ABI (ppvm_b200.PauliSum)
-  --impl reference  the CPU restatement of the reference PauliSum (oracle/) on the host,
-                    on a bounded layer prefix of the same workload (rank 0 only)
+  --impl reference  the CPU restatement of the reference PauliSum (oracle/) on every host
+                    core, one propagation of a bounded layer prefix of the same workload per
+                    core per step (rank 0 only)
 
 Multi-GPU (torchrun): every rank propagates its own replica of the circuit (the path has
 no cross-sum exchange at one sum per GPU); value = all ranks' updates / max rank time.
@@ -49,11 +50,17 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ppvm_b200", choices=["ppvm_b200", "reference"])
     ap.add_argument("--layers", type=int, default=20)
-    ap.add_argument("--workload", default="kicked_ising_2d", choices=["kicked_ising_2d", "batched_tfim", "learned_kicked_ising"],
+    ap.add_argument("--workload", default="kicked_ising_2d",
+                    choices=["kicked_ising_2d", "batched_tfim", "learned_kicked_ising", "layer_bandwidth"],
                     help="kicked_ising_2d: one 12x12 sum (headline); batched_tfim: 256 independent 1D TFIM "
                          "instances through the batched engine; learned_kicked_ising: time to <O> within 1e-3 "
-                         "with learned vs plain term-budget truncation on a 10x10 kicked-Ising circuit")
+                         "with learned vs plain term-budget truncation on a 10x10 kicked-Ising circuit; "
+                         "layer_bandwidth: the 12x12 circuit at --thr/--max-weight, one line per layer with "
+                         "each kernel family's time and algorithmic bandwidth (sums larger than L2)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--thr", type=float, default=1e-7, help="layer_bandwidth: coefficient threshold")
+    ap.add_argument("--max-weight", type=int, default=12, help="layer_bandwidth: weight cap")
+    ap.add_argument("--stop-terms", type=float, default=4e7, help="layer_bandwidth: stop past this many terms")
     return ap.parse_args()
 
 
@@ -719,8 +726,46 @@ def run_learned(args):
     print(json.dumps(line), flush=True)
 
 
+def run_layer_bandwidth(args):
+    """Kicked Ising 12x12 at a looser truncation, layer by layer: per kernel family, the
+    per-launch CUDA-event time and the algorithmic bytes (from the per-op log), for layers
+    entering with more than 2e6 terms.  Not a bench line: a measurement of the kernels on
+    sums far larger than L2."""
+    import torch
+
+    from ppvm_b200 import learned
+    from ppvm_b200.paulisum import PauliSum, ops_array
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    wl = C.kicked_ising_2d(L=12, layers=20, theta_h=0.6, thr=args.thr, max_weight=args.max_weight)
+    lay = [ops_array(p) for p in learned.split_layers(wl.ops)]
+    s = PauliSum([wl.observable[0][0]], wl.n_qubits, [1.0], min_abs_coeff=args.thr,
+                 max_pauli_weight=args.max_weight, clifford_angles=True, capacity=1 << 20)
+    for li, a in enumerate(lay):
+        n_in = len(s)
+        big = n_in > 2_000_000
+        s.profile(big)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        s.run(a)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t
+        line = {"layer": li, "terms_in": n_in, "terms_out": len(s), "wall_ms": 1e3 * wall}
+        if big:
+            line["families"] = {k: {"ms": v["ms"], "bytes": v["bytes"], "gb_s": v["bytes"] / 1e6 / max(v["ms"], 1e-9)}
+                                for k, v in s.profile_read().items() if v["launches"]}
+        print(json.dumps(line), flush=True)
+        if len(s) > args.stop_terms or n_in > args.stop_terms:
+            break
+
+
 def main():
     args = parse()
+    if args.workload == "layer_bandwidth":
+        run_layer_bandwidth(args)
+        return
     if args.workload == "learned_kicked_ising":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned truncation"}))

@@ -50,6 +50,7 @@ struct Ctrl {
   unsigned long long cap_needed;
   unsigned long long fb_cut;   // fused-run fallback: gates at the head of the run to apply one at a time, 0 = none
   unsigned long long done;     // blocks of the current launch that finished (last_block_done)
+  unsigned long long scr_top;  // fused run in scratch mode: group outputs placed in the scratch so far
 };
 
 // Per-op counters recorded for the term-gate-updates metric and the roofline bytes.

@@ -86,11 +86,12 @@ struct ProfLaunch {
 
 enum Family {
   F_SCAN = 0, F_PAIR, F_APPLY, F_COMMIT, F_CLIFF, F_TRUNC, F_READ,
-  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_GROUPS, F_TABLEAU, F_COUNT
+  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_GROUPS, F_RUN_PLACE, F_TABLEAU, F_COUNT
 };
 const char* kFamilyNames[F_COUNT] = {"rot_scan", "rot_pair", "rot_apply", "rot_commit",
                                      "clifford", "truncate", "readout",
-                                     "run_classify", "run_order", "run_scatter", "run_groups", "tableau"};
+                                     "run_classify", "run_order", "run_scatter", "run_groups", "run_place",
+                                     "tableau"};
 
 // One pinned host chunk and its device twin: per-call uploads (op descriptors, run
 // descriptors, tableaux) are packed here and copied with truly asynchronous copies.
@@ -126,6 +127,7 @@ struct ppvm_sum {
 
   uint64_t* planes = nullptr;  // x[W*cap] z[W*cap] c[cap]
   uint64_t* alt = nullptr;     // second plane buffer: fused runs write here, then swap
+  uint64_t* scr = nullptr;     // fused runs in scratch mode: group outputs before placement (cap terms)
   RunScratch R = {};
   unsigned long long* tstate2 = nullptr;
   std::vector<int> swaps;      // op indices of fused runs enqueued in the current attempt
@@ -139,6 +141,7 @@ struct ppvm_sum {
   unsigned long long run_slots_used = 0;  // group-table slots the fused runs since the last clean state hashed into
   unsigned long long* tstate = nullptr;
   unsigned long long tstate_cap = 0;
+  unsigned long long scr_cap = 0;  // capacity scr was allocated for
   uint64_t* side = nullptr;
   Ctrl* d_ctrl = nullptr;
   Ctrl* h_ctrl = nullptr;
@@ -258,6 +261,22 @@ void pool_free(void* p) {
 void destroy_now(ppvm_sum* s);                 // frees a sum and everything it holds
 ppvm_sum* take_cached(int device, int W);      // a cached sum of that device and width, or null
 
+// Fused runs with at least this many groups take scratch mode (k_run_place).  Below it the
+// per-group look-back is cheaper than the extra placement pass.  PPVM_RUN_SCRATCH_MIN_GROUPS
+// overrides it (the tests set it low, so that small sums take the scratch path too).
+unsigned long long run_scratch_min_groups() {
+  static const unsigned long long v = [] {
+    const char* e = std::getenv("PPVM_RUN_SCRATCH_MIN_GROUPS");
+    if (e && *e) {
+      char* end = nullptr;
+      const unsigned long long x = std::strtoull(e, &end, 10);
+      if (end && *end == 0) return std::max<unsigned long long>(x, 1);
+    }
+    return 1ull << 18;
+  }();
+  return v;
+}
+
 unsigned long long next_pow2(unsigned long long v) {
   unsigned long long p = 1;
   while (p < v) p <<= 1;
@@ -277,6 +296,8 @@ ppvm_status ensure_device(int dev) {
 
 void free_scratch(ppvm_sum* s) {
   pool_free(s->alt);
+  pool_free(s->scr);
+  s->scr = nullptr;
   pool_free(s->tstate2);
   uint32_t* run_arrays[] = {s->R.gslot, s->R.grp_min, s->R.grp_cnt, s->R.grp_ord, s->R.g_start,
                             s->R.g_cnt, s->R.g_rep, s->R.g_fill, s->R.mcoord};
@@ -493,7 +514,12 @@ uint64_t launch_bytes(const ppvm_sum* s, const ProfLaunch& L, const std::vector<
     }
     case F_RUN_GROUPS: {                                       // members read, group outputs written
       const OpLog& last = s->h_log[L.op + std::max(L.nops, 1) - 1];
-      return g.n_s * B + (L.nops > 1 ? last.n_s : 0) * B;
+      return (g.n_s & ~kRunLogScratchBit) * B + (L.nops > 1 ? last.n_s : 0) * B;
+    }
+    case F_RUN_PLACE: {  // scratch mode: group outputs read from the scratch, written to their place
+      if (!(g.n_s & kRunLogScratchBit)) return 0;  // look-back mode: the kernel returned at once
+      const OpLog& last = s->h_log[L.op + std::max(L.nops, 1) - 1];
+      return 2ull * (L.nops > 1 ? last.n_s : 0) * B;
     }
     default: return 0;
   }
@@ -819,11 +845,30 @@ struct K {
       ProfScope ps(s, F_RUN_SCATTER, op0, L);
       launch(k_run_scatter<W>, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, d_rd, s->R);
     }
+    // Many groups: scratch mode (group outputs placed by k_run_place, one look-back per tile
+    // of groups instead of one per group).  ngroups <= live terms <= nub, so below the
+    // threshold the device takes look-back mode and k_run_place is not needed.
+    const unsigned long long smin = run_scratch_min_groups();
+    const bool allow = nub >= smin;
+    if (allow && (!s->scr || s->scr_cap != s->cap)) {
+      pool_free(s->scr);
+      s->scr = nullptr;
+      if (pool_malloc((void**)&s->scr, sizeof(uint64_t) * (size_t)(2 * s->W + 1) * s->cap) != cudaSuccess)
+        return fail(PPVM_ECAPACITY, "device allocation failed (fused-run scratch)");
+      s->scr_cap = s->cap;
+    }
+    const Planes S = allow ? s->view_of(s->scr) : O;
+    const unsigned long long scratch_min = allow ? smin : ~0ull;
     {
       ProfScope ps(s, F_RUN_GROUPS, op0, L);
       launch(k_run_groups<W>, grid_for(nub, kRunWarps, 8), kRunWarps * 32, 0, s->stream,
-          P, O, s->d_ctrl, d_rd, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0,
-          trunc_op, s->d_log);  // its last block publishes the counts and the op log
+          O, S, s->d_ctrl, d_rd, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0,
+          trunc_op, s->d_log, scratch_min);  // its last block publishes the counts and the op log
+    }
+    if (allow) {
+      ProfScope ps(s, F_RUN_PLACE, op0, L);
+      launch(k_run_place<W, 256, 2>, grid_for(nub, 512, 4), 256, 0, s->stream,
+          S, O, s->d_ctrl, s->R, scratch_min, s->tstate, s->next_tile_epoch(), op0);
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);
@@ -975,6 +1020,7 @@ ppvm_status clear_err(ppvm_sum* s) {
   c.err_op = 0;
   c.fb_cut = 0;
   c.done = 0;  // blocks that returned early on the error never counted
+  c.scr_top = 0;
   for (int t = 0; t < 4; ++t) c.tickets[t] = 0;
   CUDA_TRY(cudaMemcpyAsync(s->d_ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));

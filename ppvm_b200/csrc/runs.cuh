@@ -29,6 +29,7 @@ namespace ppvm {
 constexpr int kRunMaxK = 10;       // groups up to 2^10 coordinates in shared memory
 constexpr int kRunMaxGates = 256;  // gates per fused run
 constexpr int kRunWarps = 4;       // groups per block tile
+constexpr unsigned long long kRunLogScratchBit = 1ull << 63;  // in the op log of a run's first gate
 constexpr int kErrFallback = 4;    // device error: a group exceeds kRunMaxK; rerun per gate
 
 struct RunDesc {
@@ -366,7 +367,8 @@ __global__ void __launch_bounds__(256) k_run_scatter(Planes P, Ctrl* ctrl, const
 // Publishes the count after the run and fills the op log of its gates (and its TRUNCATE):
 // one warp of the last block of k_run_groups.  Gate j's live count is n0 plus the children
 // the gates before it created (an exclusive scan of the created counts, 8 gates per lane).
-__device__ __forceinline__ void run_commit(Ctrl* ctrl, RunScratch R, int op0, int L, int trunc_op, OpLog* log) {
+__device__ __forceinline__ void run_commit(Ctrl* ctrl, RunScratch R, int op0, int L, int trunc_op, OpLog* log,
+                                           bool scratch, unsigned long long cap) {
   const unsigned lane = threadIdx.x & 31;
   if (ld_volatile_int(&ctrl->err)) {
     if (lane < 4) ctrl->tickets[lane] = 0;
@@ -404,9 +406,20 @@ __device__ __forceinline__ void run_commit(Ctrl* ctrl, RunScratch R, int op0, in
   __syncwarp();
   if (lane == 0) {
     const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs);
-    const unsigned long long nun = ld_volatile(&ctrl->n_s), cap_needed = ld_volatile(&ctrl->cap_needed);
+    const unsigned long long nun = ld_volatile(&ctrl->n_s);
     for (int t = 0; t < 4; ++t) ctrl->tickets[t] = 0;
-    log[op0].n_s = ld_volatile(&ctrl->n_side);  // touched terms (profiling bytes)
+    // scratch mode: the counter holds every group output; they reach O in k_run_place
+    const unsigned long long cap_needed = scratch ? nun + ld_volatile(&ctrl->scr_top) : ld_volatile(&ctrl->cap_needed);
+    if (scratch) {
+      ctrl->scr_top = 0;
+      if (cap_needed > cap) {
+        ctrl->cap_needed = cap_needed;
+        set_err(ctrl, kErrCapacity, op0);
+        return;
+      }
+    }
+    // touched terms (profiling bytes); bit 63 says the run took scratch mode
+    log[op0].n_s = ld_volatile(&ctrl->n_side) | (scratch ? kRunLogScratchBit : 0ull);
     if (L > 1) log[op0 + L - 1].n_s = (ngroups == 0) ? 0 : cap_needed - nun;  // group outputs
     const unsigned long long out = (ngroups == 0) ? nun : cap_needed;
     if (trunc_op >= 0) {
@@ -423,8 +436,9 @@ __device__ __forceinline__ void run_commit(Ctrl* ctrl, RunScratch R, int op0, in
 // which places every group's survivors after those of all lower-numbered groups.
 template <int W>
 __global__ void __launch_bounds__(kRunWarps * 32)
-k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, int trunc, double thr,
-             unsigned long long maxw, unsigned long long* ts, unsigned epoch, int op, int trunc_op, OpLog* log) {
+k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, int trunc, double thr,
+             unsigned long long maxw, unsigned long long* ts, unsigned epoch, int op, int trunc_op, OpLog* log,
+             unsigned long long scratch_min) {
   pdl_wait();
   constexpr int SZ = 1 << kRunMaxK;
   __shared__ double s_coef[kRunWarps][SZ];
@@ -446,6 +460,7 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   if (s_err) return;
   const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs);
   const unsigned long long ubase = ld_volatile(&ctrl->n_s);  // untouched survivors go first
+  const bool scratch = ngroups >= scratch_min;               // the same in every block
   const uint32_t cls = rd->cls;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool wcap = maxw != ~0ull;
@@ -551,8 +566,24 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
 #pragma unroll
     for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(kFull, mine, o);
     mine = __shfl_sync(kFull, mine, 0);
-    const unsigned long long excl = warp_lookback(ts, g, mine, epoch, ctrl, op);
-    unsigned long long out = ubase + excl;
+    // The group's output position.  Look-back mode: after all lower-numbered groups, found by
+    // a warp-level look-back.  Scratch mode (many groups): wherever a counter puts it in the
+    // scratch planes S; k_run_place then moves every group's block to its place in O.
+    unsigned long long excl = 0, out;
+    Planes D = O;
+    if (scratch) {
+      unsigned long long b = 0;
+      if (lane == 0) {
+        b = atomicAdd(&ctrl->scr_top, (unsigned long long)mine);
+        R.g_rep[g] = (uint32_t)(b < 0xFFFFFFFFull ? b : 0xFFFFFFFFull);  // scratch offset (< capacity < 2^32)
+        R.g_fill[g] = mine;                                                      // survivors
+      }
+      out = __shfl_sync(kFull, b, 0);
+      D = S;
+    } else {
+      excl = warp_lookback(ts, g, mine, epoch, ctrl, op);
+      out = ubase + excl;
+    }
     for (unsigned c0 = 0; c0 < size; c0 += 32) {
       const unsigned c = c0 + lane;
       bool keep = false;
@@ -563,7 +594,7 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
       const unsigned bal = __ballot_sync(kFull, keep);
       if (keep) {
         const unsigned long long r = out + __popc(bal & ((1u << lane) - 1u));
-        if (r < O.cap) {
+        if (r < D.cap) {
           uint64_t f[W], x[W], z[W];
 #pragma unroll
           for (int w = 0; w < W; ++w) f[w] = f0[w];
@@ -579,13 +610,13 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
             x[w] = cls == 0 ? f[w] : v[w];
             z[w] = cls == 0 ? v[w] : f[w];
           }
-          store_key<W>(O, r, x, z);
-          O.c[r] = coef[c];
+          store_key<W>(D, r, x, z);
+          D.c[r] = coef[c];
         }
       }
       out += __popc(bal);
     }
-    if (g == ngroups - 1 && lane == 0) {
+    if (!scratch && g == ngroups - 1 && lane == 0) {
       ctrl->cap_needed = ubase + excl + mine;
       if (ubase + excl + mine > O.cap) set_err(ctrl, kErrCapacity, op);
     }
@@ -594,7 +625,94 @@ k_run_groups(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   __syncthreads();
   for (unsigned j = threadIdx.x; j < L; j += blockDim.x)
     if (s_created[j]) atomicAdd(&R.created[j], s_created[j]);
-  if (last_block_done(&ctrl->done) && warp == 0) run_commit(ctrl, R, op, (int)L, trunc_op, log);
+  if (last_block_done(&ctrl->done) && warp == 0) run_commit(ctrl, R, op, (int)L, trunc_op, log, scratch, O.cap);
+}
+
+// Scratch mode of a fused run (many groups): k_run_groups left each group's survivors in a
+// contiguous block of the scratch planes S, at R.g_rep[g] (R.g_fill[g] of them).  Groups are
+// taken in tiles of BLOCK * ITEMS, in group order: one decoupled look-back per tile gives the
+// tile's output offset, a block scan the offsets of its groups, and the block's warps then
+// copy whole blocks (one term per lane) to O.  The result is the look-back mode's, term for
+// term, at one look-back per tile instead of one per group.
+template <int W, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK)
+k_run_place(Planes S, Planes O, Ctrl* ctrl, RunScratch R, unsigned long long scratch_min, unsigned long long* ts,
+            unsigned epoch, int op) {
+  pdl_wait();
+  constexpr int NW = BLOCK / 32;
+  constexpr int TILE = BLOCK * ITEMS;
+  __shared__ unsigned s_tile;
+  __shared__ unsigned long long s_slot;
+  __shared__ unsigned s_wsum[ITEMS * NW + 1];
+  __shared__ uint32_t s_src[TILE], s_cnt[TILE];
+  __shared__ unsigned long long s_dst[TILE];
+  __shared__ int s_skip;
+  if (threadIdx.x == 0) {
+    const unsigned long long ng = ld_volatile(&ctrl->n_pairs);
+    s_skip = ld_volatile_int(&ctrl->err) || ng == 0 || ng < scratch_min;
+  }
+  __syncthreads();
+  if (s_skip) return;  // the same in every block (look-back mode, or an earlier error)
+  const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs), ubase = ld_volatile(&ctrl->n_s);
+  const unsigned long long ntiles = (ngroups + TILE - 1) / TILE;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    const unsigned tile = next_tile(&ctrl->tickets[0], &s_tile);
+    if (tile >= ntiles) break;
+    const unsigned long long base = (unsigned long long)tile * TILE;
+    unsigned cnt[ITEMS], pre[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const unsigned long long gi = base + (unsigned long long)k * BLOCK + threadIdx.x;
+      cnt[k] = gi < ngroups ? R.g_fill[gi] : 0u;
+      unsigned v = cnt[k];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(kFull, v, o);
+        if (lane >= (unsigned)o) v += t;
+      }
+      pre[k] = v - cnt[k];
+      if (lane == 31) s_wsum[k * NW + warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // group order inside the tile: item k, then warp, then lane
+      unsigned run = 0;
+      for (int e = 0; e < ITEMS * NW; ++e) {
+        const unsigned t = s_wsum[e];
+        s_wsum[e] = run;
+        run += t;
+      }
+      s_wsum[ITEMS * NW] = run;
+    }
+    __syncthreads();
+    const unsigned long long excl = lookback(ts, tile, s_wsum[ITEMS * NW], epoch, ctrl, op, &s_slot);
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const unsigned long long gi = base + (unsigned long long)k * BLOCK + threadIdx.x;
+      const int q = k * BLOCK + threadIdx.x;
+      s_cnt[q] = cnt[k];
+      s_src[q] = gi < ngroups ? R.g_rep[gi] : 0u;
+      s_dst[q] = ubase + excl + s_wsum[k * NW + warp] + pre[k];
+    }
+    __syncthreads();
+    for (int q = warp; q < TILE; q += NW) {  // one group per warp, one term per lane
+      const unsigned n = s_cnt[q];
+      const unsigned long long src = s_src[q], dst = s_dst[q];
+      for (unsigned e = lane; e < n; e += 32) {
+        const unsigned long long a = src + e, b = dst + e;
+        if (a < S.cap && b < O.cap) {  // the commit checked that everything fits
+#pragma unroll
+          for (int w = 0; w < W; ++w) {
+            O.x[(unsigned long long)w * O.cap + b] = S.x[(unsigned long long)w * S.cap + a];
+            O.z[(unsigned long long)w * O.cap + b] = S.z[(unsigned long long)w * S.cap + a];
+          }
+          O.c[b] = S.c[a];
+        }
+      }
+    }
+    __syncthreads();  // the tile arrays are rewritten by the block's next tile
+  }
+  if (last_block_done(&ctrl->done) && threadIdx.x == 0) ctrl->tickets[0] = 0;
 }
 
 }  // namespace ppvm
