@@ -494,7 +494,8 @@ struct ProfScope {
   }
 };
 
-// Algorithmic bytes of one launch, from the op log ("roofline").
+// Algorithmic bytes of one launch, from the op log: the bytes the launch must move at least
+// (B = 16W + 8 per term: X and Z planes and the coefficient), the numerator of its roofline.
 uint64_t launch_bytes(const ppvm_sum* s, const ProfLaunch& L, const std::vector<int>& test_words) {
   const uint64_t B = 16ull * s->W + 8;
   const OpLog& g = s->h_log[L.op];
