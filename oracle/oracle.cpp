@@ -1,10 +1,19 @@
 // oracle/oracle.cpp — TEST INFRASTRUCTURE ONLY.
 //
 // A CPU restatement of the reference's PauliSum hot path (QuEraComputing/ppvm,
-// crate `ppvm-pauli-sum` with the IndexMap + FxHash config that the Python binding
-// uses, crates/ppvm-python-native/src/interface.rs:414).  It is the checker the GPU
-// engine is compared against and the CPU baseline that bench.py times.  Nothing in
-// the product (ppvm_b200/) links, loads or calls it.
+// crate `ppvm-pauli-sum`).  It is the checker the GPU engine is compared against and
+// the CPU baseline that bench.py times.  Nothing in the product (ppvm_b200/) links,
+// loads or calls it.
+//
+// Two map configurations of the reference are restated, behind the same gate code:
+//  * IndexMap + FxHash, single-threaded: the configuration the Python binding uses
+//    (crates/ppvm-python-native/src/interface.rs:414).  Term order is the reference's
+//    insertion order; every parity test compares against this one.
+//  * DashMap + FxHash with rayon (crates/ppvm-pauli-sum/src/config/dashmap.rs,
+//    crates/ppvm-traits/src/map/dashmap.rs): the reference's multi-threaded
+//    configuration, restated with a pool of host threads.  Same terms and coefficients (a merged key
+//    takes at most two contributions per gate, so the sum does not depend on order);
+//    term order is per-shard.  bench.py's reference arm times it on every host core.
 //
 // The reference is Rust and cannot be compiled in this environment (no cargo/rustc),
 // so this file restates it.  It is pinned by the reference's own golden values and
@@ -15,27 +24,36 @@
 // state-vector check of Heisenberg propagation.
 //
 // Semantics restated (file:line in the reference):
-//  * storage: an insertion-ordered map word -> f64 (IndexMap).  New keys append;
-//    `+=` on an existing key modifies in place (crates/ppvm-traits/src/map/hashmap.rs:40-44);
-//    `retain` keeps order (hashmap.rs:242-258 -> IndexMap::retain).
+//  * storage: a map word -> f64.  IndexMap: new keys append; `+=` on an existing key
+//    modifies in place (crates/ppvm-traits/src/map/hashmap.rs:40-44); `retain` keeps
+//    order (hashmap.rs:242-258 -> IndexMap::retain).
 //  * rotations: map_insert (crates/ppvm-pauli-sum/src/sum/data.rs:204-226): every
 //    anticommuting parent is scaled in place by cos and its child (word, v*(eps*sin)) is
-//    pushed to a scratch Vec in iteration order; then the scratch is merged with `+=`.
+//    pushed to a scratch Vec in iteration order; then the scratch is merged with `+=`,
+//    one key after the other.
 //  * Cliffords: scale (in place, data.rs:192-197) for X/Y/Z; map_add (data.rs:255-265,
-//    hashmap.rs:46-54) — a full rebuild into the aux map in iteration order — for the rest.
+//    hashmap.rs:46-54): aux cleared, every entry mapped into aux, data and aux swapped.
 //  * truncate: data.rs:275-311 with CombinedStrategy(CoefficientThreshold, MaxPauliWeight)
 //    (crates/ppvm-pauli-sum/src/strategy.rs:12-30, 73-90, 125-134).
 //  * trace: fold in iteration order (hashmap.rs:108-127) with the PauliPattern matcher
 //    (crates/ppvm-pauli-word/src/pattern/parse.rs:32-127, contains.rs:19-151).
 //
-// Build: `make -C oracle` (g++ -O2 -ffp-contract=off); the library is
+// Build: `make -C oracle` (g++ -O2 -ffp-contract=off -pthread); the library is
 // oracle/_build/liboracle.so.
 
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../include/ppvm_cuda.h"
@@ -47,92 +65,32 @@ constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 inline uint64_t rotl(uint64_t v, int r) { return (v << r) | (v >> (64 - r)); }
 
 // FxHash-style word hash (the reference hashes the raw storage bytes with FxHasher,
-// crates/ppvm-pauli-word/src/word/data.rs:184-200).  Only speed depends on it.
+// crates/ppvm-pauli-word/src/word/data.rs:184-200).  Only speed and the DashMap shard a
+// key lives in depend on it.
 inline uint64_t fx_hash(const uint64_t* k, int nw) {
   uint64_t h = 0;
   for (int i = 0; i < nw; ++i) h = (rotl(h, 5) ^ k[i]) * 0x517cc1b727220a95ull;
   return h ^ (h >> 32);
 }
 
-struct Pattern;
+inline uint64_t table_cap_for(size_t entries) {
+  uint64_t cap = 16;
+  while (cap < 2 * (uint64_t)entries + 2) cap <<= 1;
+  return cap;
+}
 
-struct OSum {
+// Word geometry and the strategy, shared by both map configurations.  A key is the X
+// plane's W words followed by the Z plane's W words.
+struct Words {
   uint32_t n = 0;
   int W = 1;  // words per plane
   double thr = 1e-10;
   uint64_t maxw = UINT64_MAX;
   bool clifford_angles = false;
-  std::vector<uint64_t> keys;  // [i][2W]: x words then z words
-  std::vector<double> vals;
-  std::vector<uint32_t> table;  // open addressing, slot -> entry index
-  uint64_t mask = 0;
   std::vector<uint64_t> preserve;  // flat [j][2W]
-  std::vector<uint64_t> scratch_keys;
-  std::vector<double> scratch_vals;
 
-  size_t len() const { return vals.size(); }
-  const uint64_t* key(size_t i) const { return &keys[i * 2 * W]; }
-  uint64_t* key(size_t i) { return &keys[i * 2 * W]; }
-
-  void reserve_index(size_t expected) {  // empty table sized for `expected` entries
-    uint64_t cap = 16;
-    while (cap < 2 * (uint64_t)expected + 2) cap <<= 1;
-    table.assign(cap, kEmpty);
-    mask = cap - 1;
-  }
-  void rebuild_index() {
-    reserve_index(len());
-    for (size_t i = 0; i < len(); ++i) {
-      uint64_t s = fx_hash(key(i), 2 * W) & mask;
-      while (table[s] != kEmpty) s = (s + 1) & mask;
-      table[s] = (uint32_t)i;
-    }
-  }
-  long find(const uint64_t* k) const {
-    if (table.empty()) return -1;
-    uint64_t s = fx_hash(k, 2 * W) & mask;
-    while (table[s] != kEmpty) {
-      if (std::memcmp(key(table[s]), k, sizeof(uint64_t) * 2 * W) == 0) return table[s];
-      s = (s + 1) & mask;
-    }
-    return -1;
-  }
-  // IndexMap entry(key).and_modify(|v| *v += value).or_insert(value)
-  void add_assign(const uint64_t* k, double v) {
-    long i = find(k);
-    if (i >= 0) {
-      vals[i] += v;
-      return;
-    }
-    if (table.empty() || 2 * (len() + 1) + 2 > table.size()) {
-      keys.insert(keys.end(), k, k + 2 * W);
-      vals.push_back(v);
-      rebuild_index();
-      return;
-    }
-    size_t idx = len();
-    keys.insert(keys.end(), k, k + 2 * W);
-    vals.push_back(v);
-    uint64_t s = fx_hash(k, 2 * W) & mask;
-    while (table[s] != kEmpty) s = (s + 1) & mask;
-    table[s] = (uint32_t)idx;
-  }
-  template <class F>
-  void retain(F keep) {  // stable, like IndexMap::retain
-    size_t o = 0;
-    for (size_t i = 0; i < len(); ++i) {
-      if (keep(key(i), vals[i])) {
-        if (o != i) {
-          std::memcpy(key(o), key(i), sizeof(uint64_t) * 2 * W);
-          vals[o] = vals[i];
-        }
-        ++o;
-      }
-    }
-    keys.resize(o * 2 * W);
-    vals.resize(o);
-    rebuild_index();
-  }
+  int kw() const { return 2 * W; }
+  size_t kb() const { return sizeof(uint64_t) * 2 * W; }
   bool get_x(const uint64_t* k, uint32_t q) const { return (k[q >> 6] >> (q & 63)) & 1u; }
   bool get_z(const uint64_t* k, uint32_t q) const { return (k[W + (q >> 6)] >> (q & 63)) & 1u; }
   static void set_bit(uint64_t* w, uint32_t q, bool b) {
@@ -146,57 +104,469 @@ struct OSum {
     for (int w = 0; w < W; ++w) t += __builtin_popcountll(k[w] | k[W + w]);
     return t;
   }
+};
 
-  // map_insert (data.rs:204-226): f(key, &v, child_key) -> has child, child value.
+// ---- IndexMap configuration -------------------------------------------------------------
+struct IndexStore : Words {
+  std::vector<uint64_t> keys;  // [i][2W]: x words then z words
+  std::vector<double> vals;
+  std::vector<uint32_t> table;  // open addressing, slot -> entry index
+  uint64_t mask = 0;
+  std::vector<uint64_t> scratch_keys;
+  std::vector<double> scratch_vals;
+  // aux map of map_add: kept from gate to gate, as the reference's aux.clear() keeps it
+  std::vector<uint64_t> aux_keys;
+  std::vector<double> aux_vals;
+  std::vector<uint32_t> aux_table;
+  uint64_t aux_mask = 0;
+
+  void init() { rebuild_index(); }
+  size_t len() const { return vals.size(); }
+  const uint64_t* key(size_t i) const { return &keys[i * 2 * W]; }
+  uint64_t* key(size_t i) { return &keys[i * 2 * W]; }
+
+  void reserve_index(size_t expected) {  // empty table sized for `expected` entries
+    uint64_t cap = table_cap_for(expected);
+    table.assign(cap, kEmpty);
+    mask = cap - 1;
+  }
+  void rebuild_index() {
+    reserve_index(len());
+    for (size_t i = 0; i < len(); ++i) {
+      uint64_t s = fx_hash(key(i), kw()) & mask;
+      while (table[s] != kEmpty) s = (s + 1) & mask;
+      table[s] = (uint32_t)i;
+    }
+  }
+  long find(const uint64_t* k) const {
+    if (table.empty()) return -1;
+    uint64_t s = fx_hash(k, kw()) & mask;
+    while (table[s] != kEmpty) {
+      if (std::memcmp(key(table[s]), k, kb()) == 0) return table[s];
+      s = (s + 1) & mask;
+    }
+    return -1;
+  }
+  bool get(const uint64_t* k, double& v) const {
+    long i = find(k);
+    if (i < 0) return false;
+    v = vals[i];
+    return true;
+  }
+  // IndexMap entry(key).and_modify(|v| *v += value).or_insert(value)
+  void add_assign(const uint64_t* k, double v) {
+    long i = find(k);
+    if (i >= 0) {
+      vals[i] += v;
+      return;
+    }
+    if (table.empty() || 2 * (len() + 1) + 2 > table.size()) {
+      keys.insert(keys.end(), k, k + kw());
+      vals.push_back(v);
+      rebuild_index();
+      return;
+    }
+    size_t idx = len();
+    keys.insert(keys.end(), k, k + kw());
+    vals.push_back(v);
+    uint64_t s = fx_hash(k, kw()) & mask;
+    while (table[s] != kEmpty) s = (s + 1) & mask;
+    table[s] = (uint32_t)idx;
+  }
+  template <class F>
+  void retain(F keep) {  // stable, like IndexMap::retain
+    size_t o = 0;
+    for (size_t i = 0; i < len(); ++i) {
+      if (keep(key(i), vals[i])) {
+        if (o != i) {
+          std::memcpy(key(o), key(i), kb());
+          vals[o] = vals[i];
+        }
+        ++o;
+      }
+    }
+    keys.resize(o * kw());
+    vals.resize(o);
+    rebuild_index();
+  }
+  // map_insert (data.rs:204-226): f(child_key, &v, child_value) -> has child.
   template <class F>
   void map_insert(F f) {
     scratch_keys.clear();
     scratch_vals.clear();
-    std::vector<uint64_t> ck(2 * W);
+    std::vector<uint64_t> ck(kw());
     size_t n0 = len();
     for (size_t i = 0; i < n0; ++i) {
       double cv;
-      std::memcpy(ck.data(), key(i), sizeof(uint64_t) * 2 * W);
+      std::memcpy(ck.data(), key(i), kb());
       if (f(ck.data(), vals[i], cv)) {
         scratch_keys.insert(scratch_keys.end(), ck.begin(), ck.end());
         scratch_vals.push_back(cv);
       }
     }
-    for (size_t j = 0; j < scratch_vals.size(); ++j) add_assign(&scratch_keys[j * 2 * W], scratch_vals[j]);
+    for (size_t j = 0; j < scratch_vals.size(); ++j) add_assign(&scratch_keys[j * kw()], scratch_vals[j]);
   }
-  // map_add (data.rs:255-265): rebuild into a fresh map in iteration order.
+  // map_add (data.rs:255-265, hashmap.rs:46-54): `aux.clear()`, every entry mapped and
+  // `+=`-inserted into aux in iteration order, then data and aux swap.  Clearing costs a
+  // pass over aux's index, as the reference's table clear does.
   template <class F>
   void map_add(F f) {
-    OSum aux;
-    aux.n = n; aux.W = W;
-    aux.keys.reserve(keys.size());
-    aux.vals.reserve(vals.size());
-    aux.reserve_index(len());  // aux keeps its capacity across gates (aux.clear())
-    std::vector<uint64_t> nk(2 * W);
+    aux_keys.clear();
+    aux_vals.clear();
+    uint64_t cap = table_cap_for(len());
+    if (aux_table.size() < cap) aux_table.assign(cap, kEmpty);
+    else std::fill(aux_table.begin(), aux_table.end(), kEmpty);
+    aux_mask = aux_table.size() - 1;
+    std::vector<uint64_t> nk(kw());
     for (size_t i = 0; i < len(); ++i) {
-      std::memcpy(nk.data(), key(i), sizeof(uint64_t) * 2 * W);
+      std::memcpy(nk.data(), key(i), kb());
       double v = vals[i];
       f(nk.data(), v);
-      aux.add_assign(nk.data(), v);
+      uint64_t s = fx_hash(nk.data(), kw()) & aux_mask;
+      bool merged = false;
+      while (aux_table[s] != kEmpty) {
+        if (std::memcmp(&aux_keys[(size_t)aux_table[s] * kw()], nk.data(), kb()) == 0) {
+          aux_vals[aux_table[s]] += v;
+          merged = true;
+          break;
+        }
+        s = (s + 1) & aux_mask;
+      }
+      if (!merged) {
+        aux_table[s] = (uint32_t)aux_vals.size();
+        aux_keys.insert(aux_keys.end(), nk.begin(), nk.end());
+        aux_vals.push_back(v);
+      }
     }
-    keys.swap(aux.keys);
-    vals.swap(aux.vals);
-    table.swap(aux.table);
-    mask = aux.mask;
+    keys.swap(aux_keys);
+    vals.swap(aux_vals);
+    table.swap(aux_table);
+    std::swap(mask, aux_mask);
   }
   template <class F>
   void scale(F f) {
     for (size_t i = 0; i < len(); ++i) f(key(i), vals[i]);
   }
+  template <class F>
+  void for_each(F f) const {  // iteration order
+    for (size_t i = 0; i < len(); ++i) f(key(i), vals[i]);
+  }
+  double overlap_with_zero() const {  // trace("Z?*"): fold in order over X-free words
+    double acc = 0.0;
+    for (size_t i = 0; i < len(); ++i) {
+      const uint64_t* k = key(i);
+      bool xfree = true;
+      for (int w = 0; w < W; ++w) xfree &= (k[w] == 0);
+      if (xfree) acc += vals[i];
+    }
+    return acc;
+  }
+};
+
+// A fixed pool of host threads for the DashMap configuration's parallel loops (rayon's
+// global pool in the reference).  parallel_for(count, f) runs f(0..count) over the
+// pool's threads and the caller, items handed out one at a time, and returns when all
+// are done.
+class Pool {
+ public:
+  explicit Pool(int threads) {
+    for (int i = 1; i < threads; ++i) workers_.emplace_back([this] { loop(); });
+  }
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    start_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+  template <class F>
+  void parallel_for(long count, F f) {
+    std::function<void(long)> job = f;
+    if (workers_.empty() || count <= 1) {
+      for (long i = 0; i < count; ++i) job(i);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = &job;
+      total_ = count;
+      next_.store(0);
+      pending_ = (int)workers_.size();
+      ++epoch_;
+    }
+    start_.notify_all();
+    drain(job);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void drain(const std::function<void(long)>& job) {
+    for (long i; (i = next_.fetch_add(1)) < total_;) job(i);
+  }
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(long)>* job;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        start_.wait(lk, [&] { return stop_ || epoch_ != seen; });
+        if (stop_) return;
+        seen = epoch_;
+        job = job_;
+      }
+      drain(*job);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex mu_;
+  std::condition_variable start_, done_;
+  const std::function<void(long)>* job_ = nullptr;
+  long total_ = 0;
+  std::atomic<long> next_{0};
+  int pending_ = 0;
+  uint64_t epoch_ = 0;
+  bool stop_ = false;
+};
+
+
+// ---- DashMap configuration ----------------------------------------------------------------
+// DashMap keeps 4 x (hardware threads) shards, rounded up to a power of two; a key lives
+// in the shard its hash selects, and each shard is a lock-guarded hash map.  The rayon
+// operations of crates/ppvm-traits/src/map/dashmap.rs run over the shards in parallel:
+// scale (par_iter_mut, :194-210), map_add_assign (par_iter, each output inserted under
+// its shard's lock, :46-55), map_insert_vec (par_extend of the parents' children in shard
+// order, :158-166) and trace (par_iter filter + sum, :96-113).  `retain` walks the shards
+// one after another (DashMap::retain, :222-227), and PauliSum::map_insert merges the
+// scratch Vec one key at a time (data.rs:221-223), so truncation and the child merge of a
+// rotation stay serial, as in the reference.
+struct ShardStore : Words {
+  // Each shard on cache lines of its own, as DashMap pads its shards: two threads that fill
+  // different shards then never write the same line.
+  struct alignas(128) Shard {
+    std::vector<uint64_t> keys;
+    std::vector<double> vals;
+    std::vector<uint32_t> table;
+    uint64_t mask = 0;
+  };
+  int threads = 1;
+  int shard_bits = 0;
+  std::vector<Shard> data, aux;
+  struct alignas(128) Lock {
+    std::atomic<uint32_t> held{0};
+  };
+  std::unique_ptr<Lock[]> locks;  // one per shard of the map being filled
+  std::unique_ptr<Pool> pool;
+  std::vector<std::vector<uint64_t>> child_keys;    // per shard: the rotation's children
+  std::vector<std::vector<double>> child_vals;
+
+  ShardStore() = default;
+  ShardStore(const ShardStore& o)
+      : Words(o), threads(o.threads), shard_bits(o.shard_bits), data(o.data), aux(o.aux),
+        child_keys(o.child_keys), child_vals(o.child_vals) {
+    make_locks();
+    pool.reset(new Pool(threads));
+  }
+
+  size_t shards() const { return data.size(); }
+  void make_locks() {
+    locks.reset(new Lock[shards()]);
+  }
+  void init() {
+    if (threads < 1) threads = 1;
+    size_t s = 1;
+    while (s < 4 * (size_t)threads) s <<= 1;
+    shard_bits = 0;
+    while ((1ull << shard_bits) < s) ++shard_bits;
+    data.assign(s, Shard());
+    aux.assign(s, Shard());
+    for (auto& sh : data) reset(sh, 0);
+    for (auto& sh : aux) reset(sh, 0);
+    child_keys.assign(s, {});
+    child_vals.assign(s, {});
+    make_locks();
+    pool.reset(new Pool(threads));
+  }
+  // bits 40.. of the hash pick the shard, the low bits the slot inside it
+  size_t shard_of(uint64_t h) const { return (size_t)(h >> 40) & (shards() - 1); }
+  void reset(Shard& sh, size_t expected) {
+    uint64_t cap = table_cap_for(expected);
+    if (sh.table.size() < cap) sh.table.assign(cap, kEmpty);
+    else std::fill(sh.table.begin(), sh.table.end(), kEmpty);
+    sh.mask = sh.table.size() - 1;
+    sh.keys.clear();
+    sh.vals.clear();
+  }
+  void reindex(Shard& sh) const {
+    uint64_t cap = table_cap_for(sh.vals.size());
+    sh.table.assign(cap, kEmpty);
+    sh.mask = cap - 1;
+    for (size_t i = 0; i < sh.vals.size(); ++i) {
+      uint64_t s = fx_hash(&sh.keys[i * kw()], kw()) & sh.mask;
+      while (sh.table[s] != kEmpty) s = (s + 1) & sh.mask;
+      sh.table[s] = (uint32_t)i;
+    }
+  }
+  long find_in(const Shard& sh, const uint64_t* k, uint64_t h) const {
+    uint64_t s = h & sh.mask;
+    while (sh.table[s] != kEmpty) {
+      if (std::memcmp(&sh.keys[(size_t)sh.table[s] * kw()], k, kb()) == 0) return sh.table[s];
+      s = (s + 1) & sh.mask;
+    }
+    return -1;
+  }
+  // entry(key).and_modify(+=).or_insert into one shard (the caller holds its lock)
+  void insert_in(Shard& sh, const uint64_t* k, double v, uint64_t h) const {
+    long i = find_in(sh, k, h);
+    if (i >= 0) {
+      sh.vals[i] += v;
+      return;
+    }
+    sh.keys.insert(sh.keys.end(), k, k + kw());
+    sh.vals.push_back(v);
+    if (2 * sh.vals.size() + 2 > sh.table.size()) {
+      reindex(sh);
+      return;
+    }
+    uint64_t s = h & sh.mask;
+    while (sh.table[s] != kEmpty) s = (s + 1) & sh.mask;
+    sh.table[s] = (uint32_t)(sh.vals.size() - 1);
+  }
+
+  size_t len() const {
+    size_t t = 0;
+    for (const auto& sh : data) t += sh.vals.size();
+    return t;
+  }
+  bool get(const uint64_t* k, double& v) const {
+    uint64_t h = fx_hash(k, kw());
+    const Shard& sh = data[shard_of(h)];
+    long i = find_in(sh, k, h);
+    if (i < 0) return false;
+    v = sh.vals[i];
+    return true;
+  }
+  void add_assign(const uint64_t* k, double v) {  // single caller: the shard lock is free
+    uint64_t h = fx_hash(k, kw());
+    insert_in(data[shard_of(h)], k, v, h);
+  }
+  template <class F>
+  void retain(F keep) {  // shard after shard (DashMap::retain)
+    for (auto& sh : data) {
+      size_t o = 0;
+      for (size_t i = 0; i < sh.vals.size(); ++i) {
+        if (keep(&sh.keys[i * kw()], sh.vals[i])) {
+          if (o != i) {
+            std::memcpy(&sh.keys[o * kw()], &sh.keys[i * kw()], kb());
+            sh.vals[o] = sh.vals[i];
+          }
+          ++o;
+        }
+      }
+      sh.keys.resize(o * kw());
+      sh.vals.resize(o);
+      reindex(sh);
+    }
+  }
+  template <class F>
+  void map_insert(F f) {
+    const long S = (long)shards();
+    pool->parallel_for(S, [&](long s) {
+      Shard& sh = data[s];
+      auto& ok = child_keys[s];
+      auto& ov = child_vals[s];
+      ok.clear();
+      ov.clear();
+      std::vector<uint64_t> ck(kw());
+      const size_t n0 = sh.vals.size();
+      for (size_t i = 0; i < n0; ++i) {
+        double cv;
+        std::memcpy(ck.data(), &sh.keys[i * kw()], kb());
+        if (f(ck.data(), sh.vals[i], cv)) {
+          ok.insert(ok.end(), ck.begin(), ck.end());
+          ov.push_back(cv);
+        }
+      }
+    });
+    for (long s = 0; s < S; ++s)  // the scratch Vec, merged one key after the other
+      for (size_t j = 0; j < child_vals[s].size(); ++j) add_assign(&child_keys[s][j * kw()], child_vals[s][j]);
+  }
+  template <class F>
+  void map_add(F f) {
+    const long S = (long)shards();
+    size_t expect = len() / shards() + 1;
+    for (auto& sh : aux) reset(sh, expect);  // aux.clear(): capacity kept
+    pool->parallel_for(S, [&](long s) {
+      const Shard& sh = data[s];
+      std::vector<uint64_t> nk(kw());
+      for (size_t i = 0; i < sh.vals.size(); ++i) {
+        std::memcpy(nk.data(), &sh.keys[i * kw()], kb());
+        double v = sh.vals[i];
+        f(nk.data(), v);
+        uint64_t h = fx_hash(nk.data(), kw());
+        size_t d = shard_of(h);
+        uint32_t z = 0;
+        while (!locks[d].held.compare_exchange_weak(z, 1u, std::memory_order_acquire)) z = 0;
+        insert_in(aux[d], nk.data(), v, h);
+        locks[d].held.store(0u, std::memory_order_release);
+      }
+    });
+    data.swap(aux);
+  }
+  template <class F>
+  void scale(F f) {
+    const long S = (long)shards();
+    pool->parallel_for(S, [&](long s) {
+      Shard& sh = data[s];
+      for (size_t i = 0; i < sh.vals.size(); ++i) f(&sh.keys[i * kw()], sh.vals[i]);
+    });
+  }
+  template <class F>
+  void for_each(F f) const {
+    for (const auto& sh : data)
+      for (size_t i = 0; i < sh.vals.size(); ++i) f(&sh.keys[i * kw()], sh.vals[i]);
+  }
+  double overlap_with_zero() const {  // per-shard partial sums, added in shard order
+    const long S = (long)shards();
+    std::vector<double> part(S, 0.0);
+    pool->parallel_for(S, [&](long s) {
+      const Shard& sh = data[s];
+      double acc = 0.0;
+      for (size_t i = 0; i < sh.vals.size(); ++i) {
+        const uint64_t* k = &sh.keys[i * kw()];
+        bool xfree = true;
+        for (int w = 0; w < W; ++w) xfree &= (k[w] == 0);
+        if (xfree) acc += sh.vals[i];
+      }
+      part[s] = acc;
+    });
+    double acc = 0.0;
+    for (long s = 0; s < S; ++s) acc += part[s];
+    return acc;
+  }
+};
+
+// ---- gates, noise and truncation over either map ------------------------------------------
+template <class M>
+struct Sum : M {
+  using M::W;
+  using M::get_x;
+  using M::get_z;
+  using M::set_x;
+  using M::set_z;
 
   // ---- Clifford gates (crates/ppvm-pauli-sum/src/sum/clifford.rs) ------------------
-  void g_x(uint32_t q) { scale([&](const uint64_t* k, double& v) { if (get_z(k, q)) v *= -1.0; }); }
-  void g_y(uint32_t q) { scale([&](const uint64_t* k, double& v) { if (get_x(k, q) ^ get_z(k, q)) v *= -1.0; }); }
-  void g_z(uint32_t q) { scale([&](const uint64_t* k, double& v) { if (get_x(k, q)) v *= -1.0; }); }
+  void g_x(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (get_z(k, q)) v *= -1.0; }); }
+  void g_y(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (get_x(k, q) ^ get_z(k, q)) v *= -1.0; }); }
+  void g_z(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (get_x(k, q)) v *= -1.0; }); }
   // single-qubit map_add gates: mode selects the bit map and the sign rule.
   enum Single { H, S, SDAG, SQX, SQXDAG, SQY, SQYDAG };
   void g_single(Single g, uint32_t q) {
-    map_add([&](uint64_t* k, double& v) {
+    this->map_add([&](uint64_t* k, double& v) {
       bool x = get_x(k, q), z = get_z(k, q);
       bool neg = false;
       switch (g) {
@@ -214,7 +584,7 @@ struct OSum {
   // two-qubit map_word! gates via PhasedPauliWord (crates/ppvm-pauli-word/src/phase/clifford.rs:72-100,168-182)
   enum Two { CNOT, CZ, CY };
   void g_two(Two g, uint32_t c, uint32_t t) {
-    map_add([&](uint64_t* k, double& v) {
+    this->map_add([&](uint64_t* k, double& v) {
       bool xc = get_x(k, c), zc = get_z(k, c), xt = get_x(k, t), zt = get_z(k, t);
       bool neg = false;
       switch (g) {
@@ -238,7 +608,7 @@ struct OSum {
   // ---- rotations (crates/ppvm-pauli-sum/src/sum/rot1.rs:55-128, rot2.rs:63-184) -----
   // Each closure mirrors the reference fast path: parent *= cos; child = v * (eps * sin).
   void r_x(uint32_t q, double s, double co) {
-    map_insert([&](uint64_t* k, double& v, double& cv) {
+    this->map_insert([&](uint64_t* k, double& v, double& cv) {
       if (!get_z(k, q)) return false;
       bool xb = get_x(k, q);
       double coeff = v;
@@ -250,7 +620,7 @@ struct OSum {
     });
   }
   void r_y(uint32_t q, double s, double co) {
-    map_insert([&](uint64_t* k, double& v, double& cv) {
+    this->map_insert([&](uint64_t* k, double& v, double& cv) {
       bool xb = get_x(k, q), zb = get_z(k, q);
       if (xb == zb) return false;
       double coeff = v;
@@ -262,7 +632,7 @@ struct OSum {
     });
   }
   void r_z(uint32_t q, double s, double co) {
-    map_insert([&](uint64_t* k, double& v, double& cv) {
+    this->map_insert([&](uint64_t* k, double& v, double& cv) {
       bool xb = get_x(k, q);
       if (!xb) return false;
       bool zb = get_z(k, q);
@@ -275,7 +645,7 @@ struct OSum {
     });
   }
   void r_zz(uint32_t a, uint32_t b, double s, double co) {
-    map_insert([&](uint64_t* k, double& v, double& cv) {
+    this->map_insert([&](uint64_t* k, double& v, double& cv) {
       bool xa = get_x(k, a), xb = get_x(k, b);
       if (xa == xb) return false;
       bool za = get_z(k, a), zb = get_z(k, b);
@@ -289,7 +659,7 @@ struct OSum {
     });
   }
   void r_xx(uint32_t a, uint32_t b, double s, double co) {
-    map_insert([&](uint64_t* k, double& v, double& cv) {
+    this->map_insert([&](uint64_t* k, double& v, double& cv) {
       bool za = get_z(k, a), zb = get_z(k, b);
       if (za == zb) return false;
       bool xa = get_x(k, a), xb = get_x(k, b);
@@ -303,7 +673,7 @@ struct OSum {
     });
   }
   void r_yy(uint32_t a, uint32_t b, double s, double co) {
-    map_insert([&](uint64_t* k, double& v, double& cv) {
+    this->map_insert([&](uint64_t* k, double& v, double& cv) {
       bool xa = get_x(k, a), za = get_z(k, a), xb = get_x(k, b), zb = get_z(k, b);
       bool pa = xa ^ za, pb = xb ^ zb;
       if (pa == pb) return false;
@@ -342,7 +712,7 @@ struct OSum {
   }
   // Generic exp(-i theta/2 G): rotate_1 / rotate_2 generalised to any support.
   void r_pauli(const uint64_t* gx, const uint64_t* gz, double s, double co) {
-    map_insert([&](uint64_t* k, double& v, double& cv) {
+    this->map_insert([&](uint64_t* k, double& v, double& cv) {
       if (!anticommutes(gx, gz, k)) return false;
       double eps = (double)rot_sign(gx, gz, k);
       double coeff = v;
@@ -356,7 +726,7 @@ struct OSum {
   // P -> sign * (iGP), a bijection on words.  Tests pin it against the reference's
   // Clifford compositions (e.g. RZZ(-pi/2) == CZ, S_DAG, S_DAG).
   void r_pauli_clifford(const uint64_t* gx, const uint64_t* gz, double sin_sign) {
-    map_add([&](uint64_t* k, double& v) {
+    this->map_add([&](uint64_t* k, double& v) {
       if (!anticommutes(gx, gz, k)) return;
       double eps = (double)rot_sign(gx, gz, k);
       for (int w = 0; w < W; ++w) { k[w] ^= gx[w]; k[W + w] ^= gz[w]; }
@@ -370,18 +740,18 @@ struct OSum {
     double xf = one - p[1] * 2.0 - p[2] * 2.0;
     double zf = one - p[0] * 2.0 - p[1] * 2.0;
     double yf = one - p[0] * 2.0 - p[2] * 2.0;
-    scale([&](const uint64_t* k, double& v) {
+    this->scale([&](const uint64_t* k, double& v) {
       int code = (int)get_x(k, q) | ((int)get_z(k, q) << 1);
       if (code == 1) v *= xf; else if (code == 2) v *= zf; else if (code == 3) v *= yf;
     });
   }
   void depolarize1(uint32_t q, double p) {  // noise.rs:107-116
     double f = 1.0 - p * (4.0 / 3.0);
-    scale([&](const uint64_t* k, double& v) { if (get_x(k, q) | get_z(k, q)) v *= f; });
+    this->scale([&](const uint64_t* k, double& v) { if (get_x(k, q) | get_z(k, q)) v *= f; });
   }
   void depolarize2(uint32_t a, uint32_t b, double p) {  // noise.rs:119-129
     double f = 1.0 - p * (16.0 / 15.0);
-    scale([&](const uint64_t* k, double& v) {
+    this->scale([&](const uint64_t* k, double& v) {
       if (get_x(k, a) | get_z(k, a) | get_x(k, b) | get_z(k, b)) v *= f;
     });
   }
@@ -408,7 +778,7 @@ struct OSum {
           for (int t = 0; t < 8; ++t) acc = acc - p[kIdx[ca][cb][t]] * 2.0;
         f[ca][cb] = acc;
       }
-    scale([&](const uint64_t* k, double& v) {
+    this->scale([&](const uint64_t* k, double& v) {
       const int ca = (int)get_x(k, a) | ((int)get_z(k, a) << 1);
       const int cb = (int)get_x(k, b) | ((int)get_z(k, b) << 1);
       if (ca | cb) v *= f[ca][cb];
@@ -419,7 +789,7 @@ struct OSum {
   void amplitude_damping(uint32_t q, double gamma) {
     const double om = 1.0 - gamma;
     const double sxy = std::sqrt(om);
-    map_insert([&](uint64_t* ck, double& v, double& cv) {
+    this->map_insert([&](uint64_t* ck, double& v, double& cv) {
       if (get_x(ck, q)) {
         v *= sxy;
         return false;
@@ -434,39 +804,30 @@ struct OSum {
 
   // ---- truncation (data.rs:275-311, strategy.rs) -------------------------------------
   void strategy() {
-    double t = thr;
-    retain([&](const uint64_t*, double v) { return !(std::fabs(v) < t); });  // strategy.rs:125-134
-    if (maxw != UINT64_MAX) {  // strategy.rs:86-90
-      uint64_t mw = maxw;
-      retain([&](const uint64_t* k, double) { return weight(k) <= mw; });
+    double t = this->thr;
+    this->retain([&](const uint64_t*, double v) { return !(std::fabs(v) < t); });  // strategy.rs:125-134
+    if (this->maxw != UINT64_MAX) {  // strategy.rs:86-90
+      uint64_t mw = this->maxw;
+      this->retain([&](const uint64_t* k, double) { return this->weight(k) <= mw; });
     }
   }
   bool is_preserved(const uint64_t* k) const {
-    size_t np = preserve.size() / (2 * W);
+    size_t np = this->preserve.size() / (2 * W);
     for (size_t j = 0; j < np; ++j)
-      if (std::memcmp(&preserve[j * 2 * W], k, sizeof(uint64_t) * 2 * W) == 0) return true;
+      if (std::memcmp(&this->preserve[j * 2 * W], k, this->kb()) == 0) return true;
     return false;
   }
   void truncate() {
-    if (preserve.empty()) { strategy(); return; }
+    if (this->preserve.empty()) { strategy(); return; }
     std::vector<uint64_t> sk;
     std::vector<double> sv;
-    for (size_t i = 0; i < len(); ++i)
-      if (is_preserved(key(i))) { sk.insert(sk.end(), key(i), key(i) + 2 * W); sv.push_back(vals[i]); }
+    this->for_each([&](const uint64_t* k, double v) {
+      if (is_preserved(k)) { sk.insert(sk.end(), k, k + 2 * W); sv.push_back(v); }
+    });
     strategy();
+    double dummy;
     for (size_t j = 0; j < sv.size(); ++j)
-      if (find(&sk[j * 2 * W]) < 0) add_assign(&sk[j * 2 * W], sv[j]);
-  }
-
-  double overlap_with_zero() const {  // trace("Z?*"): fold in order over X-free words
-    double acc = 0.0;
-    for (size_t i = 0; i < len(); ++i) {
-      const uint64_t* k = key(i);
-      bool xfree = true;
-      for (int w = 0; w < W; ++w) xfree &= (k[w] == 0);
-      if (xfree) acc += vals[i];
-    }
-    return acc;
+      if (!this->get(&sk[j * 2 * W], dummy)) this->add_assign(&sk[j * 2 * W], sv[j]);
   }
 };
 
@@ -525,7 +886,7 @@ Pattern parse_pattern(const char* s) {  // parse.rs:32-127
   return P;
 }
 // contains.rs:120-151 (match_position :44-66, match_star :68-84, match_repeat :86-116)
-bool pattern_contains(const Pattern& P, const OSum& S, const uint64_t* k) {
+bool pattern_contains(const Pattern& P, const Words& S, const uint64_t* k) {
   uint32_t pos = 0, n = S.n;
   auto code = [&](uint32_t q) { return (unsigned)S.get_x(k, q) | ((unsigned)S.get_z(k, q) << 1); };
   auto accepts = [](unsigned acc, unsigned c) { return (acc >> (c == 0 ? 0 : c == 1 ? 1 : c == 2 ? 2 : 3)) & 1u; };
@@ -562,11 +923,11 @@ bool pattern_contains(const Pattern& P, const OSum& S, const uint64_t* k) {
   return true;
 }
 
-thread_local std::string g_err;
+bool qok(const Words* s, uint32_t q) { return q < s->n; }
 
-bool qok(const OSum* s, uint32_t q) { return q < s->n; }
-
-int run_op(OSum* s, const ppvm_op& op) {
+template <class M>
+int run_op(Sum<M>* s, const ppvm_op& op) {
+  using SumT = Sum<M>;
   const double HALF_PI = 1.5707963267948966;
   auto two_ok = [&]() { return qok(s, op.q0) && qok(s, op.q1) && op.q0 != op.q1; };
   auto is_cliff_angle = [&](double th) { return s->clifford_angles && (th == HALF_PI || th == -HALF_PI); };
@@ -579,16 +940,16 @@ int run_op(OSum* s, const ppvm_op& op) {
     case PPVM_OP_X: if (!qok(s, op.q0)) return 1; s->g_x(op.q0); return 0;
     case PPVM_OP_Y: if (!qok(s, op.q0)) return 1; s->g_y(op.q0); return 0;
     case PPVM_OP_Z: if (!qok(s, op.q0)) return 1; s->g_z(op.q0); return 0;
-    case PPVM_OP_H: if (!qok(s, op.q0)) return 1; s->g_single(OSum::H, op.q0); return 0;
-    case PPVM_OP_S: if (!qok(s, op.q0)) return 1; s->g_single(OSum::S, op.q0); return 0;
-    case PPVM_OP_S_DAG: if (!qok(s, op.q0)) return 1; s->g_single(OSum::SDAG, op.q0); return 0;
-    case PPVM_OP_SQRT_X: if (!qok(s, op.q0)) return 1; s->g_single(OSum::SQX, op.q0); return 0;
-    case PPVM_OP_SQRT_X_DAG: if (!qok(s, op.q0)) return 1; s->g_single(OSum::SQXDAG, op.q0); return 0;
-    case PPVM_OP_SQRT_Y: if (!qok(s, op.q0)) return 1; s->g_single(OSum::SQY, op.q0); return 0;
-    case PPVM_OP_SQRT_Y_DAG: if (!qok(s, op.q0)) return 1; s->g_single(OSum::SQYDAG, op.q0); return 0;
-    case PPVM_OP_CNOT: if (!two_ok()) return 1; s->g_two(OSum::CNOT, op.q0, op.q1); return 0;
-    case PPVM_OP_CZ: if (!two_ok()) return 1; s->g_two(OSum::CZ, op.q0, op.q1); return 0;
-    case PPVM_OP_CY: if (!two_ok()) return 1; s->g_two(OSum::CY, op.q0, op.q1); return 0;
+    case PPVM_OP_H: if (!qok(s, op.q0)) return 1; s->g_single(SumT::H, op.q0); return 0;
+    case PPVM_OP_S: if (!qok(s, op.q0)) return 1; s->g_single(SumT::S, op.q0); return 0;
+    case PPVM_OP_S_DAG: if (!qok(s, op.q0)) return 1; s->g_single(SumT::SDAG, op.q0); return 0;
+    case PPVM_OP_SQRT_X: if (!qok(s, op.q0)) return 1; s->g_single(SumT::SQX, op.q0); return 0;
+    case PPVM_OP_SQRT_X_DAG: if (!qok(s, op.q0)) return 1; s->g_single(SumT::SQXDAG, op.q0); return 0;
+    case PPVM_OP_SQRT_Y: if (!qok(s, op.q0)) return 1; s->g_single(SumT::SQY, op.q0); return 0;
+    case PPVM_OP_SQRT_Y_DAG: if (!qok(s, op.q0)) return 1; s->g_single(SumT::SQYDAG, op.q0); return 0;
+    case PPVM_OP_CNOT: if (!two_ok()) return 1; s->g_two(SumT::CNOT, op.q0, op.q1); return 0;
+    case PPVM_OP_CZ: if (!two_ok()) return 1; s->g_two(SumT::CZ, op.q0, op.q1); return 0;
+    case PPVM_OP_CY: if (!two_ok()) return 1; s->g_two(SumT::CY, op.q0, op.q1); return 0;
     case PPVM_OP_RX: case PPVM_OP_RY: case PPVM_OP_RZ: {
       if (!qok(s, op.q0)) return 1;
       bool gxb = op.code != PPVM_OP_RZ, gzb = op.code != PPVM_OP_RX;
@@ -626,32 +987,85 @@ int run_op(OSum* s, const ppvm_op& op) {
   }
 }
 
+// One handle type for both configurations: the C functions below dispatch on it.
+struct Handle {
+  virtual ~Handle() = default;
+  virtual Handle* clone() const = 0;
+  virtual Words& words() = 0;
+  virtual size_t len() const = 0;
+  virtual void add_assign(const uint64_t* k, double v) = 0;
+  virtual int run(const ppvm_op& op) = 0;
+  virtual void two_qubit_pauli_error(uint32_t a, uint32_t b, const double* p) = 0;
+  virtual void truncate() = 0;
+  virtual void rotation(const uint64_t* gx, const uint64_t* gz, double theta) = 0;
+  virtual double overlap_with_zero() const = 0;
+  virtual void each(const std::function<void(const uint64_t*, double)>& f) const = 0;
+  virtual bool get(const uint64_t* k, double& v) const = 0;
+};
+
+template <class M>
+struct HandleT : Handle {
+  Sum<M> s;
+  Handle* clone() const override { return new HandleT(*this); }
+  Words& words() override { return s; }
+  size_t len() const override { return s.len(); }
+  void add_assign(const uint64_t* k, double v) override { s.add_assign(k, v); }
+  int run(const ppvm_op& op) override { return run_op(&s, op); }
+  void two_qubit_pauli_error(uint32_t a, uint32_t b, const double* p) override { s.two_qubit_pauli_error(a, b, p); }
+  void truncate() override { s.truncate(); }
+  void rotation(const uint64_t* gx, const uint64_t* gz, double theta) override {
+    const double HALF_PI = 1.5707963267948966;
+    if (s.clifford_angles && (theta == HALF_PI || theta == -HALF_PI)) {
+      s.r_pauli_clifford(gx, gz, theta > 0 ? 1.0 : -1.0);
+      return;
+    }
+    s.r_pauli(gx, gz, std::sin(theta), std::cos(theta));
+  }
+  double overlap_with_zero() const override { return s.overlap_with_zero(); }
+  void each(const std::function<void(const uint64_t*, double)>& f) const override { s.for_each(f); }
+  bool get(const uint64_t* k, double& v) const override { return s.get(k, v); }
+};
+
+template <class M>
+Handle* make_handle(uint32_t n, double thr, uint64_t maxw, uint32_t flags, int threads) {
+  auto* h = new HandleT<M>();
+  Sum<M>& s = h->s;
+  s.n = n;
+  s.W = (int)((n + 63) / 64);
+  s.thr = thr;
+  s.maxw = maxw;
+  s.clifford_angles = (flags & PPVM_FLAG_CLIFFORD_ANGLES) != 0;
+  if constexpr (std::is_same<M, ShardStore>::value) s.threads = threads;
+  s.init();
+  return h;
+}
+
 }  // namespace
 
 extern "C" {
 
 void* oracle_create(uint32_t n, double thr, uint64_t maxw, uint32_t flags) {
   if (n == 0) return nullptr;
-  OSum* s = new OSum();
-  s->n = n;
-  s->W = (int)((n + 63) / 64);
-  s->thr = thr;
-  s->maxw = maxw;
-  s->clifford_angles = (flags & PPVM_FLAG_CLIFFORD_ANGLES) != 0;
-  s->rebuild_index();
-  return s;
+  return make_handle<IndexStore>(n, thr, maxw, flags, 1);
 }
-void oracle_destroy(void* h) { delete (OSum*)h; }
-void* oracle_clone(void* h) { return new OSum(*(OSum*)h); }
-int oracle_words(void* h) { return ((OSum*)h)->W; }
-size_t oracle_len(void* h) { return ((OSum*)h)->len(); }
+// The DashMap configuration on `threads` threads (0: every hardware thread).
+void* oracle_create_sharded(uint32_t n, double thr, uint64_t maxw, uint32_t flags, int threads) {
+  if (n == 0) return nullptr;
+  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  return make_handle<ShardStore>(n, thr, maxw, flags, threads);
+}
+void oracle_destroy(void* h) { delete (Handle*)h; }
+void* oracle_clone(void* h) { return ((Handle*)h)->clone(); }
+int oracle_words(void* h) { return ((Handle*)h)->words().W; }
+size_t oracle_len(void* h) { return ((Handle*)h)->len(); }
 
 // x, z term-major [k][W]
 int oracle_add_terms(void* h, const uint64_t* x, const uint64_t* z, const double* c, size_t k) {
-  OSum* s = (OSum*)h;
-  std::vector<uint64_t> key(2 * s->W);
+  Handle* s = (Handle*)h;
+  const int W = s->words().W;
+  std::vector<uint64_t> key(2 * W);
   for (size_t i = 0; i < k; ++i) {
-    for (int w = 0; w < s->W; ++w) { key[w] = x[i * s->W + w]; key[s->W + w] = z[i * s->W + w]; }
+    for (int w = 0; w < W; ++w) { key[w] = x[i * W + w]; key[W + w] = z[i * W + w]; }
     s->add_assign(key.data(), c[i]);
   }
   return 0;
@@ -659,73 +1073,72 @@ int oracle_add_terms(void* h, const uint64_t* x, const uint64_t* z, const double
 // two_qubit_pauli_error_many: pairs (flat, k_flat even) in order, then the strategy if asked.
 int oracle_two_qubit_pauli_error(void* h, const uint32_t* pairs, size_t k_flat, const double* p,
                                  int truncate) {
-  OSum* s = (OSum*)h;
+  Handle* s = (Handle*)h;
+  const uint32_t n = s->words().n;
   if (k_flat % 2) return 1;
   for (size_t i = 0; i < k_flat; i += 2)
-    if (pairs[i] >= s->n || pairs[i + 1] >= s->n || pairs[i] == pairs[i + 1]) return 1;
+    if (pairs[i] >= n || pairs[i + 1] >= n || pairs[i] == pairs[i + 1]) return 1;
   for (size_t i = 0; i < k_flat; i += 2) s->two_qubit_pauli_error(pairs[i], pairs[i + 1], p);
   if (truncate) s->truncate();
   return 0;
 }
 int oracle_set_preserve(void* h, const uint64_t* x, const uint64_t* z, size_t k) {
-  OSum* s = (OSum*)h;
-  s->preserve.clear();
+  Words& s = ((Handle*)h)->words();
+  s.preserve.clear();
   for (size_t i = 0; i < k; ++i) {
-    for (int w = 0; w < s->W; ++w) s->preserve.push_back(x[i * s->W + w]);
-    for (int w = 0; w < s->W; ++w) s->preserve.push_back(z[i * s->W + w]);
+    for (int w = 0; w < s.W; ++w) s.preserve.push_back(x[i * s.W + w]);
+    for (int w = 0; w < s.W; ++w) s.preserve.push_back(z[i * s.W + w]);
   }
   return 0;
 }
 // Runs ops in order; records the live count entering each op into counts (may be NULL).
 int oracle_run_ops(void* h, const ppvm_op* ops, size_t n_ops, uint64_t* counts) {
-  OSum* s = (OSum*)h;
+  Handle* s = (Handle*)h;
   for (size_t i = 0; i < n_ops; ++i) {
     if (counts) counts[i] = s->len();
-    if (run_op(s, ops[i]) != 0) return (int)(i + 1);
+    if (s->run(ops[i]) != 0) return (int)(i + 1);
   }
   return 0;
 }
 int oracle_pauli_rotation(void* h, const uint64_t* gx, const uint64_t* gz, double theta) {
-  OSum* s = (OSum*)h;
-  const double HALF_PI = 1.5707963267948966;
-  if (s->clifford_angles && (theta == HALF_PI || theta == -HALF_PI)) {
-    s->r_pauli_clifford(gx, gz, theta > 0 ? 1.0 : -1.0);
-    return 0;
-  }
-  s->r_pauli(gx, gz, std::sin(theta), std::cos(theta));
+  ((Handle*)h)->rotation(gx, gz, theta);
   return 0;
 }
-double oracle_overlap_with_zero(void* h) { return ((OSum*)h)->overlap_with_zero(); }
+double oracle_overlap_with_zero(void* h) { return ((Handle*)h)->overlap_with_zero(); }
 int oracle_trace(void* h, const char* pattern, double* out) {
-  OSum* s = (OSum*)h;
+  Handle* s = (Handle*)h;
   Pattern P = parse_pattern(pattern);
   if (!P.ok) return 1;
   double acc = 0.0;
-  for (size_t i = 0; i < s->len(); ++i)
-    if (pattern_contains(P, *s, s->key(i))) acc += s->vals[i];
+  const Words& w = s->words();
+  s->each([&](const uint64_t* k, double v) {
+    if (pattern_contains(P, w, k)) acc += v;
+  });
   *out = acc;
   return 0;
 }
 // PauliSum::overlap (sum/trace.rs:31-37): other.iter().map(|(k,v)| v * self[k]).sum()
 double oracle_overlap(void* a, void* b) {
-  OSum* A = (OSum*)a;
-  OSum* B = (OSum*)b;
+  Handle* A = (Handle*)a;
+  Handle* B = (Handle*)b;
   double acc = 0.0;
-  for (size_t i = 0; i < B->len(); ++i) {
-    long j = A->find(B->key(i));
-    acc += B->vals[i] * (j >= 0 ? A->vals[j] : 0.0);
-  }
+  B->each([&](const uint64_t* k, double v) {
+    double av;
+    acc += v * (A->get(k, av) ? av : 0.0);
+  });
   return acc;
 }
 size_t oracle_export(void* h, uint64_t* x, uint64_t* z, double* c, size_t cap) {
-  OSum* s = (OSum*)h;
-  size_t n = s->len() < cap ? s->len() : cap;
-  for (size_t i = 0; i < n; ++i) {
-    const uint64_t* k = s->key(i);
-    for (int w = 0; w < s->W; ++w) { x[i * s->W + w] = k[w]; z[i * s->W + w] = k[s->W + w]; }
-    c[i] = s->vals[i];
-  }
-  return n;
+  Handle* s = (Handle*)h;
+  const int W = s->words().W;
+  size_t i = 0;
+  s->each([&](const uint64_t* k, double v) {
+    if (i >= cap) return;
+    for (int w = 0; w < W; ++w) { x[i * W + w] = k[w]; z[i * W + w] = k[W + w]; }
+    c[i] = v;
+    ++i;
+  });
+  return i;
 }
 
 }  // extern "C"

@@ -49,6 +49,8 @@ def lib():
         PD = ctypes.POINTER(ctypes.c_double)
         L.oracle_create.restype = vp
         L.oracle_create.argtypes = [u32, dbl, u64, u32]
+        L.oracle_create_sharded.restype = vp
+        L.oracle_create_sharded.argtypes = [u32, dbl, u64, u32, ctypes.c_int]
         L.oracle_destroy.argtypes = [vp]
         L.oracle_clone.restype = vp
         L.oracle_clone.argtypes = [vp]
@@ -97,14 +99,23 @@ def ops_to_struct(ops) -> ctypes.Array:
 
 
 class OracleSum:
-    """The reference PauliSum semantics on the CPU (insertion-ordered map)."""
+    """The reference PauliSum semantics on the CPU.
+
+    By default the IndexMap configuration (insertion-ordered map, one thread), the one every
+    parity test compares against.  ``threads`` selects the reference's DashMap configuration
+    instead, on that many host threads (0: all): the same terms and coefficients, in
+    per-shard order."""
 
     def __init__(self, n_qubits: int, min_abs_coeff: float = 1e-10,
-                 max_weight: int | None = None, clifford_angles: bool = False):
+                 max_weight: int | None = None, clifford_angles: bool = False, threads: int | None = None):
         L = lib()
         self.n = n_qubits
         mw = (1 << 64) - 1 if max_weight is None else int(max_weight)
-        self._h = L.oracle_create(n_qubits, min_abs_coeff, mw, 1 if clifford_angles else 0)
+        flags = 1 if clifford_angles else 0
+        if threads is None:
+            self._h = L.oracle_create(n_qubits, min_abs_coeff, mw, flags)
+        else:
+            self._h = L.oracle_create_sharded(n_qubits, min_abs_coeff, mw, flags, int(threads))
         if not self._h:
             raise ValueError("oracle_create failed")
         self.W = L.oracle_words(self._h)

@@ -119,11 +119,15 @@ def kicked_ising_random_h(L: int = 10, layers: int = 30, seed: int = 2, lo: floa
     return wl
 
 
-def clifford_t(n: int = 64, layers: int = 1000, seed: int = 0, p_t: float = 0.05, thr: float = 1e-6) -> Workload:
+def clifford_t(n: int = 64, layers: int = 1000, seed: int = 0, p_t: float = 0.05, thr: float = 1e-6,
+               heisenberg_layers: int | None = None) -> Workload:
     """Random Clifford+T brickwork.  Forward layer: each qubit one of {H, S, S_DAG}; CNOT on
     (2i, 2i+1) for even layers, (2i+1, 2i+2) for odd ones; then T = RZ(pi/4) on each qubit with
     probability p_t.  Observable: a random weight-4 Pauli.  Heisenberg order, TRUNCATE after
-    each layer's T block (Cliffords keep |c|, so a truncate after them is a no-op)."""
+    each layer's T block (Cliffords keep |c|, so a truncate after them is a no-op).
+
+    ``heisenberg_layers`` = k keeps only the first k layers of the Heisenberg list (the last k
+    forward layers): a prefix of the same ``layers``-layer circuit, observable included."""
     rng = SplitMix64(seed)
     fwd_layers = []
     for layer in range(layers):
@@ -140,13 +144,20 @@ def clifford_t(n: int = 64, layers: int = 1000, seed: int = 0, p_t: float = 0.05
     word = ["I"] * n
     for q in qs:
         word[q] = "XYZ"[rng.below(3)]
+    kept = list(reversed(fwd_layers))
+    if heisenberg_layers is not None:
+        kept = kept[:heisenberg_layers]
     ops = []
-    for singles, pairs, ts in reversed(fwd_layers):
+    for singles, pairs, ts in kept:
         ops += [G.r1(G.RZ, q, math.pi / 4) for q in reversed(ts)] + [G.truncate()]
         ops += [G.g2(G.CNOT, a, b) for a, b in reversed(pairs)]
         ops += [G.g1(code, q) for q, code in reversed(list(enumerate(singles)))]
-    return Workload(f"clifford_t_n{n}_layers{layers}_seed{seed}", n, thr, None, [("".join(word), 1.0)], ops,
-                    meta={"layers": layers, "seed": seed, "t_gates": sum(len(t) for _, _, t in fwd_layers)})
+    name = f"clifford_t_n{n}_layers{layers}_seed{seed}"
+    if heisenberg_layers is not None:
+        name += f"_first{len(kept)}"
+    return Workload(name, n, thr, None, [("".join(word), 1.0)], ops,
+                    meta={"layers": layers, "seed": seed, "heisenberg_layers": len(kept),
+                          "t_gates": sum(len(t) for _, _, t in kept)})
 
 
 def batched_tfim(count: int = 256, seed: int = 1, thr: float = 1e-5) -> list[Workload]:

@@ -1,5 +1,6 @@
 """The bench's reference arms on the CPU: each prints one JSON line with the fields of the
-bench contract (a short layer prefix keeps the headline arm to seconds)."""
+bench contract, and the same ``config`` the GPU arm prints for that workload (a 2-layer
+kicked-Ising circuit keeps the headline arm to seconds here)."""
 
 import json
 import os
@@ -28,10 +29,38 @@ def _check(d):
     assert d["e2e"]["d2h_bytes_per_step"] == 0 and "workload" in d["config"]
 
 
+def _gpu_arm_config(workload, layers=20):
+    sys.path.insert(0, ROOT)
+    import bench
+
+    return bench.config_dict(bench.workload(workload, layers), 1)
+
+
 def test_reference_arm_line():
-    d = _line("--impl", "reference", "--steps", "1", "--warmup", "0", "--layers", "2")
+    d = _line("--impl", "reference", "--steps", "1", "--warmup", "1", "--layers", "2")
     _check(d)
     assert d["unit"] == d["metric"] == "term-gate updates/s"
+    assert d["config"] == _gpu_arm_config("kicked_ising_2d", 2)
+    assert d["config"]["layers"] == 2 and d["config"]["gates_per_step"] == 2 * (264 + 144)
+    assert d["result"]["term_gate_updates_per_step"] > 0
+
+
+def test_tfim_reference_arm_line():
+    d = _line("--workload", "tfim_1d", "--impl", "reference", "--steps", "2", "--warmup", "1")
+    _check(d)
+    assert d["config"] == _gpu_arm_config("tfim_1d")
+    assert d["result"]["term_gate_updates_per_step"] == 64033
+
+
+def test_clifford_t_workload_is_a_prefix_of_the_1000_layer_circuit():
+    sys.path.insert(0, ROOT)
+    import bench
+    from ppvm_b200 import circuits as C
+
+    wl = bench.workload("clifford_t")
+    full = C.clifford_t(n=64, layers=1000, seed=0, p_t=0.05, thr=1e-6)
+    assert wl.observable == full.observable and wl.ops == full.ops[:len(wl.ops)]
+    assert bench.config_dict(wl, 1)["layers"] == 26
 
 
 def test_batched_reference_arm_line():
