@@ -5,7 +5,7 @@
  * QuEraComputing/ppvm.  Every entry point below names the reference interface it
  * replaces (paths are relative to the ppvm repository).  The reference binds this
  * path through PyO3 (`crates/ppvm-python-native/src/interface.rs`); a Rust crate
- * or a Python ctypes shim binds these symbols instead (see INTEGRATION.md).
+ * or a Python ctypes shim binds these symbols instead.
  *
  * Conventions
  *  - A Pauli word over n qubits is two bit planes of W = ceil(n/64) u64 words:
@@ -194,10 +194,11 @@ ppvm_status ppvm_overlap(ppvm_sum* a, ppvm_sum* b, double* out);
  *   cuda_stream  stream the work is queued on (NULL: the default stream); asynchronous
  * Allocates nothing: its working memory is a fixed 32 KiB array compiled into the library,
  * held on every GPU that loads the library until the process exits.  Limit: n_terms <=
- * 16,777,216 (one partial sum per 4096 terms); larger inputs return PPVM_EINVAL.  The first
- * call on each device looks up that array's device address; make that first call before any
- * stream capture.  All calls on a device share the array: calls whose kernels overlap on
- * the GPU (unordered streams) race and may return wrong sums. */
+ * 16,777,216 (one partial sum per 4096 terms); larger inputs return PPVM_EINVAL.  Every
+ * call looks up that array's device address on the current device (a lookup that allocates
+ * nothing); the first call on a device may also load the library's device code, so make
+ * that first call before any stream capture.  All calls on a device share the array: calls
+ * whose kernels overlap on the GPU (unordered streams) race and may return wrong sums. */
 ppvm_status ppvm_overlap_with_zero_noalloc(const uint64_t* d_x, size_t x_stride, uint32_t n_words,
                                            const double* d_c, size_t n_terms, double* d_out,
                                            void* cuda_stream);

@@ -51,6 +51,8 @@ struct Ctrl {
   unsigned long long fb_cut;   // fused-run fallback: gates at the head of the run to apply one at a time, 0 = none
   unsigned long long done;     // blocks of the current launch that finished (last_block_done)
   unsigned long long scr_top;  // fused run in scratch mode: group outputs placed in the scratch so far
+  unsigned spin_limit;         // polls a look-back waits before it gives up; 0 = kSpinLimit
+  unsigned reserved;
 };
 
 // Per-op counters recorded for the term-gate-updates metric and the roofline bytes.
@@ -128,6 +130,12 @@ constexpr int kValueBits = 42;
 constexpr unsigned long long kValueMask = (1ull << kValueBits) - 1;
 constexpr unsigned kSpinLimit = 1u << 22;
 
+// The poll bound of a look-back: the control block's spin_limit, or kSpinLimit when it is 0.
+__device__ __forceinline__ unsigned spin_limit_of(const Ctrl* ctrl) {
+  const unsigned v = ctrl->spin_limit;
+  return v ? v : kSpinLimit;
+}
+
 __device__ __forceinline__ unsigned long long pack_state(unsigned epoch, unsigned flag,
                                                           unsigned long long v) {
   return ((unsigned long long)(epoch & 0xFFFFFu) << 44) | ((unsigned long long)flag << 42) |
@@ -136,7 +144,10 @@ __device__ __forceinline__ unsigned long long pack_state(unsigned epoch, unsigne
 
 // Exclusive prefix of tile `tile` given its aggregate.  All threads of the block call it;
 // warp 0 publishes and looks back.  Every wait is bounded; on timeout the error flag is set
-// and a (wrong) prefix is returned so that the kernel ends.
+// and a (wrong) prefix is returned so that the kernel ends.  That prefix is the sum of the
+// non-negative aggregates read before the wait gave up, never more than the true prefix, so
+// every output offset derived from it stays at or below its true value: writes stay inside
+// the buffers sized for the true outputs.
 static __device__ unsigned long long lookback(unsigned long long* ts, unsigned tile,
                                        unsigned long long agg, unsigned epoch, Ctrl* ctrl,
                                        int op, unsigned long long* s_slot) {
@@ -149,6 +160,7 @@ static __device__ unsigned long long lookback(unsigned long long* ts, unsigned t
       if (lane == 0) st_release(&ts[tile], pack_state(epoch, 1, agg));
       long long pred = (long long)tile - 1 - (long long)lane;
       unsigned spins = 0;
+      const unsigned lim = spin_limit_of(ctrl);
       const unsigned ep = epoch & 0xFFFFFu;
       while (true) {
         unsigned flag;
@@ -163,7 +175,7 @@ static __device__ unsigned long long lookback(unsigned long long* ts, unsigned t
             val = 0;
           }
           if (__all_sync(kFull, flag != 0)) break;
-          if (++spins > kSpinLimit) {
+          if (++spins > lim) {
             if (lane == 0) set_err(ctrl, kErrTimeout, op);
             flag = 2;
             val = 0;
@@ -207,6 +219,7 @@ __device__ __forceinline__ unsigned long long warp_lookback(unsigned long long* 
   if (lane == 0) st_release(&ts[tile], pack_state(epoch, 1, agg));
   long long pred = (long long)tile - 1 - (long long)lane;
   unsigned spins = 0;
+  const unsigned lim = spin_limit_of(ctrl);
   while (true) {
     unsigned flag;
     unsigned long long val;
@@ -220,7 +233,7 @@ __device__ __forceinline__ unsigned long long warp_lookback(unsigned long long* 
         val = 0;
       }
       if (__all_sync(kFull, flag != 0)) break;
-      if (++spins > kSpinLimit) {
+      if (++spins > lim) {
         if (lane == 0) set_err(ctrl, kErrTimeout, op);
         flag = 2;
         val = 0;

@@ -46,6 +46,13 @@ ppvm_status fail(ppvm_status s, const std::string& msg) {
                   std::string(#expr) + ": " + cudaGetErrorString(e_));                   \
   } while (0)
 
+// Calls that read a sum's terms refuse a sum that an earlier failure left unusable (its
+// planes and live count may be partial): they return the same status as the ops do.
+#define REQUIRE_USABLE(s)                                                                \
+  do {                                                                                   \
+    if ((s)->poisoned) return fail(PPVM_ECUDA, "sum is in an error state from an earlier failure"); \
+  } while (0)
+
 #define PPVM_TRY(expr)                  \
   do {                                  \
     ppvm_status s_ = (expr);            \
@@ -222,7 +229,29 @@ void pool_release_device(int dev) {  // caller holds g_pool_mu; dev is current
   g_pool_free[dev].clear();
 }
 
-cudaError_t pool_malloc(void** out, size_t bytes) {
+// Where a pool allocation is made, for the allocation-failure test hook below.
+enum AllocSite : unsigned { kAllocCreate = 0, kAllocGrowth = 1, kAllocRunScratch = 2 };
+
+// Test hook: PPVM_TEST_FAIL_ALLOC names allocation sites ("growth": storage growth of a live
+// sum; "run-scratch": the fused runs' scratch planes; comma-separated) whose pool
+// allocations fail as if the device had no memory left, without calling cudaMalloc.  Read
+// once per process; the failure-handling tests set it in a child process.
+bool alloc_fails(AllocSite site) {
+  static const unsigned mask = [] {
+    unsigned m = 0;
+    const char* e = std::getenv("PPVM_TEST_FAIL_ALLOC");
+    if (e) {
+      const std::string v(e);
+      if (v.find("growth") != std::string::npos) m |= 1u << kAllocGrowth;
+      if (v.find("run-scratch") != std::string::npos) m |= 1u << kAllocRunScratch;
+    }
+    return m;
+  }();
+  return (mask >> site) & 1u;
+}
+
+cudaError_t pool_malloc(void** out, size_t bytes, AllocSite site = kAllocCreate) {
+  if (alloc_fails(site)) return cudaErrorMemoryAllocation;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -275,6 +304,31 @@ unsigned long long run_scratch_min_groups() {
     return 1ull << 18;
   }();
   return v;
+}
+
+// Polls a look-back waits for its predecessors before it gives up with PPVM_ETIMEOUT.  0 (the
+// default) leaves the device's bound of 2^22 polls; PPVM_SPIN_LIMIT overrides it, read once
+// per process (the timeout test sets a few polls, so that a multi-tile look-back gives up).
+unsigned spin_limit_setting() {
+  static const unsigned v = [] {
+    const char* e = std::getenv("PPVM_SPIN_LIMIT");
+    if (e && *e) {
+      char* end = nullptr;
+      const unsigned long long x = std::strtoull(e, &end, 10);
+      if (end && *end == 0) return (unsigned)std::min<unsigned long long>(x, 0xFFFFFFFFull);
+    }
+    return 0u;
+  }();
+  return v;
+}
+
+// The control block of a new or reused sum: all zero but the look-back poll bound.
+ppvm_status init_ctrl(ppvm_sum* s, unsigned long long n) {
+  std::memset(s->h_ctrl, 0, sizeof(Ctrl));
+  s->h_ctrl->n = n;
+  s->h_ctrl->spin_limit = spin_limit_setting();
+  CUDA_TRY(cudaMemcpyAsync(s->d_ctrl, s->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, s->stream));
+  return PPVM_OK;
 }
 
 unsigned long long next_pow2(unsigned long long v) {
@@ -336,8 +390,9 @@ ppvm_status clear_run_tables(ppvm_sum* s, unsigned long long slots) {
 ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   if (new_cap >= 0xFFFFFFF0ull) return fail(PPVM_ECAPACITY, "term capacity limit (2^32) exceeded");
   const int W = s->W;
+  const AllocSite site = s->planes ? kAllocGrowth : kAllocCreate;
   uint64_t* np = nullptr;
-  CUDA_TRY(pool_malloc((void**)&np, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&np, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap, site));
   if (s->planes) {
     for (int w = 0; w < 2 * W + 1; ++w)
       CUDA_TRY(cudaMemcpyAsync(np + (size_t)w * new_cap, s->planes + (size_t)w * s->cap,
@@ -348,34 +403,34 @@ ppvm_status grow(ppvm_sum* s, unsigned long long new_cap) {
   s->planes = np;
   s->cap = new_cap;
   free_scratch(s);
-  CUDA_TRY(pool_malloc((void**)&s->s_idx, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->partner, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->s_rec, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->s_idx, sizeof(uint32_t) * new_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->partner, sizeof(uint32_t) * new_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->s_rec, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap, site));
   s->table_cap = next_pow2(std::max<unsigned long long>(2 * new_cap, 1024));
-  CUDA_TRY(pool_malloc((void**)&s->table, sizeof(unsigned long long) * s->table_cap));
+  CUDA_TRY(pool_malloc((void**)&s->table, sizeof(unsigned long long) * s->table_cap, site));
   CUDA_TRY(cudaMemsetAsync(s->table, 0, sizeof(unsigned long long) * s->table_cap, s->stream));
   s->table_epoch = 0;
   // one tile-state word per look-back tile: the smallest tile is k_run_groups' kRunWarps groups
   s->tstate_cap = new_cap + 64;  // one tile-state word per group of a fused run at most
-  CUDA_TRY(pool_malloc((void**)&s->tstate, sizeof(unsigned long long) * s->tstate_cap));
+  CUDA_TRY(pool_malloc((void**)&s->tstate, sizeof(unsigned long long) * s->tstate_cap, site));
   CUDA_TRY(cudaMemsetAsync(s->tstate, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
-  CUDA_TRY(pool_malloc((void**)&s->tstate2, sizeof(unsigned long long) * s->tstate_cap));
+  CUDA_TRY(pool_malloc((void**)&s->tstate2, sizeof(unsigned long long) * s->tstate_cap, site));
   CUDA_TRY(cudaMemsetAsync(s->tstate2, 0, sizeof(unsigned long long) * s->tstate_cap, s->stream));
   s->tile_epoch = 0;
-  CUDA_TRY(pool_malloc((void**)&s->alt, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.gslot, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.grp_min, sizeof(uint32_t) * s->table_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.grp_cnt, sizeof(uint32_t) * s->table_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.grp_ord, sizeof(uint32_t) * s->table_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.g_start, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.g_cnt, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.g_rep, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.g_fill, sizeof(uint32_t) * new_cap));
-  CUDA_TRY(pool_malloc((void**)&s->R.mcoord, sizeof(uint32_t) * new_cap));
+  CUDA_TRY(pool_malloc((void**)&s->alt, sizeof(uint64_t) * (size_t)(2 * W + 1) * new_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.gslot, sizeof(uint32_t) * new_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.grp_min, sizeof(uint32_t) * s->table_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.grp_cnt, sizeof(uint32_t) * s->table_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.grp_ord, sizeof(uint32_t) * s->table_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.g_start, sizeof(uint32_t) * new_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.g_cnt, sizeof(uint32_t) * new_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.g_rep, sizeof(uint32_t) * new_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.g_fill, sizeof(uint32_t) * new_cap, site));
+  CUDA_TRY(pool_malloc((void**)&s->R.mcoord, sizeof(uint32_t) * new_cap, site));
   // member coefficients and group keys live in the rotation records, unused during a run
   s->R.mcoef = reinterpret_cast<double*>(s->s_rec);
   s->R.gkey = s->s_rec + new_cap;  // 2W words per group, at most new_cap groups
-  CUDA_TRY(pool_malloc((void**)&s->R.created, sizeof(unsigned long long) * kRunMaxGates));
+  CUDA_TRY(pool_malloc((void**)&s->R.created, sizeof(unsigned long long) * kRunMaxGates, site));
   return clear_run_tables(s, s->table_cap);
 }
 
@@ -849,14 +904,24 @@ struct K {
     // Many groups: scratch mode (group outputs placed by k_run_place, one look-back per tile
     // of groups instead of one per group).  ngroups <= live terms <= nub, so below the
     // threshold the device takes look-back mode and k_run_place is not needed.
+    // Scratch offsets are 32-bit (RunScratch::g_rep): scratch mode needs cap < 2^32, which
+    // grow() guarantees by refusing capacities from 0xFFFFFFF0 up.
     const unsigned long long smin = run_scratch_min_groups();
-    const bool allow = nub >= smin;
+    bool allow = nub >= smin && s->cap < 0xFFFFFFFFull;
     if (allow && (!s->scr || s->scr_cap != s->cap)) {
       pool_free(s->scr);
       s->scr = nullptr;
-      if (pool_malloc((void**)&s->scr, sizeof(uint64_t) * (size_t)(2 * s->W + 1) * s->cap) != cudaSuccess)
-        return fail(PPVM_ECAPACITY, "device allocation failed (fused-run scratch)");
-      s->scr_cap = s->cap;
+      s->scr_cap = 0;
+      if (pool_malloc((void**)&s->scr, sizeof(uint64_t) * (size_t)(2 * s->W + 1) * s->cap, kAllocRunScratch) !=
+          cudaSuccess) {
+        // no room for the scratch planes: this run takes look-back mode, which needs none
+        // (same output, slower on many groups); a later run tries the allocation again
+        cudaGetLastError();
+        s->scr = nullptr;
+        allow = false;
+      } else {
+        s->scr_cap = s->cap;
+      }
     }
     const Planes S = allow ? s->view_of(s->scr) : O;
     const unsigned long long scratch_min = allow ? smin : ~0ull;
@@ -1367,10 +1432,7 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
     for (int f = 0; f < F_COUNT; ++f) c->prof_ms[f] = 0, c->prof_launches[f] = 0, c->prof_bytes[f] = 0;
     c->launch_count = c->xfer_h2d = c->xfer_d2h = 0;
     c->last_nops = 0;
-    std::memset(c->h_ctrl, 0, sizeof(Ctrl));
-    ppvm_status st = PPVM_OK;
-    if (cudaMemsetAsync(c->d_ctrl, 0, sizeof(Ctrl), c->stream) != cudaSuccess)
-      st = fail(PPVM_ECUDA, "memset failed");
+    ppvm_status st = init_ctrl(c, 0);
     if (st == PPVM_OK && c->cap < std::max<size_t>(capacity_hint, 4096))
       st = grow(c, std::max<size_t>(capacity_hint, 4096));
     if (st == PPVM_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) st = fail(PPVM_ECUDA, "sync failed");
@@ -1402,11 +1464,11 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
       cudaMalloc(&s->d_hist, sizeof(unsigned) * 2048) != cudaSuccess ||
       cudaMalloc(&s->side, sizeof(uint64_t) * (2 * s->W + 1) * (kMaxPreserve + 1)) != cudaSuccess)
     return bail(fail(PPVM_ECAPACITY, "device allocation failed"));
-  std::memset(s->h_ctrl, 0, sizeof(Ctrl));
-  if (cudaMemsetAsync(s->d_hist, 0, sizeof(unsigned) * 2048, s->stream) != cudaSuccess ||
-      cudaMemsetAsync(s->d_ctrl, 0, sizeof(Ctrl), s->stream) != cudaSuccess)
+  if (cudaMemsetAsync(s->d_hist, 0, sizeof(unsigned) * 2048, s->stream) != cudaSuccess)
     return bail(fail(PPVM_ECUDA, "memset failed"));
-  ppvm_status st = grow(s, std::max<size_t>(capacity_hint, 4096));
+  ppvm_status st = init_ctrl(s, 0);
+  if (st != PPVM_OK) return bail(st);
+  st = grow(s, std::max<size_t>(capacity_hint, 4096));
   if (st != PPVM_OK) return bail(st);
   st = ensure_log(s, 64);
   if (st != PPVM_OK) return bail(st);
@@ -1526,6 +1588,7 @@ ppvm_status ppvm_sum_set_stream(ppvm_sum* s, void* cuda_stream) {
 
 ppvm_status ppvm_sum_clone(const ppvm_sum* src, ppvm_sum** out) {
   if (!src || !out) return fail(PPVM_EINVAL, "null argument");
+  REQUIRE_USABLE(src);
   ppvm_sum* d = nullptr;
   PPVM_TRY(ppvm_sum_create2(&d, src->n, src->thr, src->maxw, std::max<unsigned long long>(src->cap, 4096),
                             src->flags, src->device));
@@ -1536,10 +1599,7 @@ ppvm_status ppvm_sum_clone(const ppvm_sum* src, ppvm_sum** out) {
                              sizeof(uint64_t) * src->n_host, cudaMemcpyDeviceToDevice, d->stream));
   d->n_host = src->n_host;
   d->n_ub = src->n_host;
-  Ctrl c;
-  std::memset(&c, 0, sizeof(c));
-  c.n = src->n_host;
-  CUDA_TRY(cudaMemcpyAsync(d->d_ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, d->stream));
+  PPVM_TRY(init_ctrl(d, src->n_host));
   if (src->npres) {
     std::vector<uint64_t> x, z;
     for (int j = 0; j < src->npres; ++j)
@@ -1668,6 +1728,7 @@ ppvm_status ppvm_sum_set_preserve(ppvm_sum* s, const uint64_t* x, const uint64_t
 
 ppvm_status ppvm_export_terms(const ppvm_sum* cs, uint64_t* x, uint64_t* z, double* c, size_t cap, size_t* n_out) {
   if (!cs || !n_out) return fail(PPVM_EINVAL, "null argument");
+  REQUIRE_USABLE(cs);
   ppvm_sum* s = const_cast<ppvm_sum*>(cs);
   PPVM_TRY(ensure_device(s->device));
   const size_t n = std::min<size_t>(cap, s->n_host);
@@ -1692,6 +1753,7 @@ ppvm_status ppvm_export_terms(const ppvm_sum* cs, uint64_t* x, uint64_t* z, doub
 
 ppvm_status ppvm_weights(const ppvm_sum* cs, uint32_t* w, size_t cap, size_t* n_out) {
   if (!cs || !n_out) return fail(PPVM_EINVAL, "null argument");
+  REQUIRE_USABLE(cs);
   ppvm_sum* s = const_cast<ppvm_sum*>(cs);
   PPVM_TRY(ensure_device(s->device));
   const size_t n = std::min<size_t>(cap, s->n_host);
@@ -1929,6 +1991,7 @@ ppvm_status ppvm_last_run_live_counts(const ppvm_sum* s, uint64_t* counts, size_
 
 ppvm_status ppvm_overlap_with_zero(ppvm_sum* s, double* out) {
   if (!s || !out) return fail(PPVM_EINVAL, "null argument");
+  REQUIRE_USABLE(s);
   PPVM_TRY(ensure_device(s->device));
   return do_reduce_owz(s, out);
 }
@@ -1937,6 +2000,7 @@ ppvm_status ppvm_expectation(ppvm_sum* s, double* out) { return ppvm_overlap_wit
 
 ppvm_status ppvm_trace(ppvm_sum* s, const char* pattern, double* out) {
   if (!s || !pattern || !out) return fail(PPVM_EINVAL, "null argument");
+  REQUIRE_USABLE(s);
   std::vector<PatItem> items;
   if (!parse_pattern(pattern, items)) return fail(PPVM_EINVAL, std::string("bad Pauli pattern: ") + pattern);
   PPVM_TRY(ensure_device(s->device));
@@ -1957,6 +2021,8 @@ ppvm_status ppvm_trace(ppvm_sum* s, const char* pattern, double* out) {
 
 ppvm_status ppvm_overlap(ppvm_sum* a, ppvm_sum* b, double* out) {
   if (!a || !b || !out) return fail(PPVM_EINVAL, "null argument");
+  REQUIRE_USABLE(a);
+  REQUIRE_USABLE(b);
   if (a->n != b->n) return fail(PPVM_EINVAL, "sums have different qubit counts");
   if (a->device != b->device) return fail(PPVM_EINVAL, "sums live on different devices");
   PPVM_TRY(ensure_device(a->device));
@@ -1975,6 +2041,8 @@ ppvm_status ppvm_overlap(ppvm_sum* a, ppvm_sum* b, double* out) {
 
 ppvm_status ppvm_equal(const ppvm_sum* ca, const ppvm_sum* cb, int* out) {
   if (!ca || !cb || !out) return fail(PPVM_EINVAL, "null argument");
+  REQUIRE_USABLE(ca);
+  REQUIRE_USABLE(cb);
   ppvm_sum* a = const_cast<ppvm_sum*>(ca);
   ppvm_sum* b = const_cast<ppvm_sum*>(cb);
   *out = 0;
@@ -2052,6 +2120,7 @@ ppvm_status ppvm_launch_count(const ppvm_sum* s, uint64_t* out) {
 ppvm_status ppvm_term_features(ppvm_sum* s, uint32_t lattice_l, uint32_t layers_left, float* out, size_t cap,
                                size_t* n_out) {
   if (!s || !n_out) return fail(PPVM_EINVAL, "null argument");
+  REQUIRE_USABLE(s);
   if (lattice_l > 0 && (uint64_t)lattice_l * lattice_l > s->n) return fail(PPVM_EINVAL, "lattice larger than the sum");
   PPVM_TRY(ensure_device(s->device));
   const size_t n = std::min<size_t>(cap, s->n_host);

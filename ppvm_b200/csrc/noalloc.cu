@@ -17,7 +17,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "../../include/ppvm_cuda.h"
@@ -30,7 +29,6 @@ constexpr int kNaChunk = kNaBlock * kNaItems;    // terms per block (4096)
 constexpr int kNaMaxBlocks = 4096;               // partial-sum slots in the static array
 constexpr unsigned long long kNaMaxTerms = (unsigned long long)kNaChunk * kNaMaxBlocks;  // 16,777,216
 constexpr int kNaMaxWords = 8;                   // 512 qubits
-constexpr int kNaMaxDevices = 64;
 
 // The fixed working memory: one partial sum per block (32 KiB per device).
 static __device__ __align__(256) double g_na_partials[kNaMaxBlocks];
@@ -93,20 +91,17 @@ k_owz_noalloc_final(const double* partials, int nb, double* out) {
   }
 }
 
-std::mutex g_na_mu;
-double* g_na_addr[kNaMaxDevices] = {};
-
-// Device address of the static array on `dev` (the current device), looked up once.
-ppvm_status na_scratch(int dev, double** out) {
-  std::lock_guard<std::mutex> lock(g_na_mu);
-  if (!g_na_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_na_partials);
-    if (e != cudaSuccess)
-      return na_fail(PPVM_ECUDA, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-    g_na_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_na_addr[dev];
+// Device address of the static array on the current device.  Host code cannot use the
+// array's name as a device pointer (it names a host-side stand-in), so the address comes from
+// the runtime.  It is looked up on every call, not cached: the lookup allocates nothing, and
+// an address kept from before a cudaDeviceReset (or from an earlier primary context) would
+// point at freed memory.
+ppvm_status na_scratch(double** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_na_partials);
+  if (e != cudaSuccess)
+    return na_fail(PPVM_ECUDA, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+  *out = static_cast<double*>(p);
   return PPVM_OK;
 }
 
@@ -128,9 +123,8 @@ ppvm_status ppvm_overlap_with_zero_noalloc(const uint64_t* d_x, size_t x_stride,
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return na_fail(PPVM_ENODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kNaMaxDevices) return na_fail(PPVM_EINVAL, "device ordinal above 63");
   double* partials = nullptr;
-  const ppvm_status st = na_scratch(dev, &partials);
+  const ppvm_status st = na_scratch(&partials);
   if (st != PPVM_OK) return st;
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   const int nb = (int)((n_terms + kNaChunk - 1) / kNaChunk);

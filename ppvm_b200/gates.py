@@ -58,6 +58,14 @@ def pauli_error(q: int, p):
     return (PAULI_ERROR, q, 0, 0.0, tuple(float(v) for v in p))
 
 
+def depolarize1(q: int, p: float):
+    return (DEPOLARIZE1, q, 0, float(p), _ZERO3)
+
+
+def depolarize2(a: int, b: int, p: float):
+    return (DEPOLARIZE2, a, b, float(p), _ZERO3)
+
+
 def amplitude_damping(q: int, gamma: float):
     return (AMPLITUDE_DAMPING, q, 0, float(gamma), _ZERO3)
 

@@ -151,3 +151,33 @@ def test_batch_rejects_amplitude_damping():
     inst = Instance(n_qubits=4, terms=[("ZIII", 1.0)], ops=[G.amplitude_damping(0, 0.1)])
     with pytest.raises(ValueError):
         PauliSumBatch([inst])
+
+
+@pytest.mark.parametrize("exact", [True, False])
+@pytest.mark.parametrize("n", [3, 64, 65, 200])
+def test_depolarize_parity(n, exact):
+    # Depolarizing::depolarize1 / depolarize2 (crates/ppvm-pauli-sum/src/sum/noise.rs:107-129):
+    # every term with a non-identity Pauli on the target(s) is scaled, between rotations that
+    # keep the sum changing, with truncations that drop scaled terms
+    rng = np.random.default_rng(300 + n)
+    terms = random_terms(rng, n, 300)
+    hot = [int(v) for v in rng.choice(n, min(n, 8), replace=False)]
+    ops = []
+    for k in range(6):
+        a, b = hot[k % len(hot)], hot[(k + 1) % len(hot)]
+        ops += [G.r1(G.RX, a, 0.3 + 0.1 * k), G.depolarize1(a, 0.01 * (k + 1)), G.depolarize1(b, 0.2),
+                G.r2(G.RZZ, a, b, -0.4), G.depolarize2(a, b, 0.03 * (k + 1)), G.truncate()]
+    g = gpu_from(terms, n, thr=2e-3, exact=exact)
+    o = oracle_from(terms, n, thr=2e-3)
+    for i in range(0, len(ops), 6):
+        g.run(ops[i:i + 6])
+        o.run_ops(ops[i:i + 6])
+        (same if exact else same_set)(g, o)
+    # the per-gate entry points with their own truncate flag
+    g2 = gpu_from(terms, n, thr=0.05, exact=True)
+    o2 = oracle_from(terms, n, thr=0.05)
+    g2.depolarize1(hot[:3], p=0.3)
+    g2.depolarize2(hot[:4], p=0.4, truncate=False)
+    o2.run_ops([G.depolarize1(q, 0.3) for q in hot[:3]] + [G.truncate()])
+    o2.run_ops([G.depolarize2(hot[0], hot[1], 0.4), G.depolarize2(hot[2], hot[3], 0.4)])
+    same(g2, o2)

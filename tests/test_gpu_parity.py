@@ -387,3 +387,37 @@ def test_reused_handles_start_clean():
         del b
     wl = C.tfim_1d(steps=3)
     run_both(wl.observable, wl.n_qubits, wl.ops, thr=wl.min_abs_coeff, check_every=40, exact=False)
+
+
+@pytest.mark.parametrize("n", [7, 64, 100, 144, 300])
+def test_overlap_matches_oracle_on_random_sums(n):
+    # PauliSum::overlap (crates/ppvm-pauli-sum/src/sum/trace.rs:31-37): sum over the other
+    # sum's terms of its coefficient times this sum's coefficient of the same word.  Two
+    # random sums sharing about a third of their words, both propagated a little first
+    rng = np.random.default_rng(500 + n)
+
+    def words(m):
+        out = set()
+        while len(out) < m:
+            w = ["I"] * n
+            for q in rng.choice(n, int(rng.integers(1, 6)), replace=False):
+                w[int(q)] = "XYZ"[int(rng.integers(3))]
+            out.add("".join(w))
+        return sorted(out)
+
+    shared, only_a, only_b = words(300), words(400), words(200)
+    ta = [(w, float(rng.uniform(-1, 1))) for w in dict.fromkeys(shared + only_a)]
+    tb = [(w, float(rng.uniform(-1, 1))) for w in dict.fromkeys(only_b + shared)]
+    ops = [G.r1(G.RX, int(q), 0.2) for q in rng.choice(n, min(n, 5), replace=False)] + [G.truncate()]
+    for exact in (True, False):
+        ga, gb = gpu_from(ta, n, thr=1e-6, exact=exact), gpu_from(tb, n, thr=1e-6, exact=exact)
+        oa, ob = oracle_from(ta, n, thr=1e-6), oracle_from(tb, n, thr=1e-6)
+        for g, o in ((ga, oa), (gb, ob)):
+            g.run(ops)
+            o.run_ops(ops)
+        want = oa.overlap(ob)
+        assert abs(ga.overlap(gb) - want) < 1e-10, (ga.overlap(gb), want)
+        assert abs(gb.overlap(ga) - ob.overlap(oa)) < 1e-10
+        assert abs(ga.overlap(ga) - oa.overlap(oa)) < 1e-10
+    disjoint = gpu_from([("Y" * n, 1.0)], n)
+    assert ga.overlap(disjoint) == 0.0
