@@ -19,9 +19,7 @@ import json
 import os
 import subprocess
 import sys
-import tempfile
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -110,7 +108,7 @@ big.run(ops)
 o = oracle_from([("Z" * n, 1.0)], n, thr=1e-9)
 o.run_ops(ops)
 same(big, o)
-out["fresh_len"] = len(big)
+out["fresh_len"] = len(big)  # below 2^14: thr 1e-9 drops the smallest products
 print(json.dumps(out))
 """
 
@@ -119,7 +117,7 @@ def test_failed_growth_returns_ecapacity():
     r = child(GROWTH_SCRIPT, {"PPVM_TEST_FAIL_ALLOC": "growth"})
     assert r["first"] == 2, r   # PPVM_ECAPACITY
     assert r["after"] == 3, r   # PPVM_ECUDA: the sum is in an error state
-    assert r["fresh_len"] == 1 << 14, r
+    assert r["fresh_len"] > 4096, r  # more than the first sum's capacity: it had to grow
 
 
 def test_fused_runs_without_scratch_memory_fall_back_to_lookback_mode():
@@ -132,28 +130,32 @@ def test_fused_runs_without_scratch_memory_fall_back_to_lookback_mode():
 
 
 MODES_SCRIPT = r"""
-import json, sys
-import numpy as np
+import hashlib, json
 from ppvm_b200 import circuits as C
 from ppvm_b200.paulisum import PauliSum
-wl = C.kicked_ising_2d(L=12, layers=7, theta_h=0.6, thr=1e-7, max_weight=12)
+from tests.test_gpu_headline import layers_of
+wl = C.kicked_ising_2d(L=12, layers=12, theta_h=0.6, thr=1e-7, max_weight=12)
 s = PauliSum([wl.observable[0][0]], wl.n_qubits, [1.0], min_abs_coeff=wl.min_abs_coeff,
-             max_pauli_weight=wl.max_weight, clifford_angles=True, capacity=1 << 23)
-s.run(wl.ops)
+             max_pauli_weight=wl.max_weight, clifford_angles=True, capacity=1 << 22)
+max_in, counts = 0, hashlib.sha256()
+for layer in layers_of(wl.ops):
+    entering = len(s)
+    s.run(layer)
+    counts.update(s.live_counts().tobytes())
+    max_in = max(max_in, entering)
+    if entering > 2_000_000:  # that layer's RX run had far more than 2^18 groups
+        break
 x, z, c = s.export()
-np.savez(sys.argv[1], x=x, z=z, c=c, counts=s.live_counts())
-print(json.dumps({"len": len(s), "owz": s.overlap_with_zero().hex(), "max_in": int(s.live_counts().max())}))
+terms = hashlib.sha256(x.tobytes() + z.tobytes() + c.tobytes()).hexdigest()
+print(json.dumps({"len": len(s), "owz": s.overlap_with_zero().hex(), "max_in": max_in,
+                  "terms": terms, "counts": counts.hexdigest()}))
 """
 
 
 def test_scratch_mode_at_default_threshold_equals_lookback_mode():
-    with tempfile.TemporaryDirectory() as d:
-        a = child(MODES_SCRIPT.replace("sys.argv[1]", repr(os.path.join(d, "scratch.npz"))), {})
-        b = child(MODES_SCRIPT.replace("sys.argv[1]", repr(os.path.join(d, "lookback.npz"))),
-                  {"PPVM_RUN_SCRATCH_MIN_GROUPS": str(1 << 40)})
-        assert a["max_in"] > 4 << 20, a  # runs with far more than 2^18 groups took scratch mode
-        assert a == b
-        fa, fb = np.load(os.path.join(d, "scratch.npz")), np.load(os.path.join(d, "lookback.npz"))
-        for k in ("x", "z", "counts"):
-            assert np.array_equal(fa[k], fb[k]), k
-        assert np.array_equal(fa["c"].view(np.uint64), fb["c"].view(np.uint64))
+    # scratch mode places the same terms at the same positions as look-back mode: the term
+    # lists (in order), the live counts and <O> hash alike
+    a = child(MODES_SCRIPT, {})
+    b = child(MODES_SCRIPT, {"PPVM_RUN_SCRATCH_MIN_GROUPS": str(1 << 40)})
+    assert a["max_in"] > 2_000_000, a
+    assert a == b

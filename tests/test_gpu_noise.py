@@ -176,8 +176,9 @@ def test_depolarize_parity(n, exact):
     # the per-gate entry points with their own truncate flag
     g2 = gpu_from(terms, n, thr=0.05, exact=True)
     o2 = oracle_from(terms, n, thr=0.05)
+    pairs = hot[:4] if len(hot) >= 4 else hot[:2]
     g2.depolarize1(hot[:3], p=0.3)
-    g2.depolarize2(hot[:4], p=0.4, truncate=False)
+    g2.depolarize2(pairs, p=0.4, truncate=False)
     o2.run_ops([G.depolarize1(q, 0.3) for q in hot[:3]] + [G.truncate()])
-    o2.run_ops([G.depolarize2(hot[0], hot[1], 0.4), G.depolarize2(hot[2], hot[3], 0.4)])
+    o2.run_ops([G.depolarize2(pairs[i], pairs[i + 1], 0.4) for i in range(0, len(pairs), 2)])
     same(g2, o2)
