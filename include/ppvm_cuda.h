@@ -56,6 +56,9 @@ typedef enum ppvm_opcode {
   PPVM_OP_DEPOLARIZE2,                                   /* q0, q1, theta = p */
   PPVM_OP_TRUNCATE,                                      /* run the strategy */
   PPVM_OP_AMPLITUDE_DAMPING,                             /* q0, theta = gamma */
+  PPVM_OP_LOSS_CHANNEL,                                  /* q0, theta = p (lossy sums) */
+  PPVM_OP_RESET_LOSS_CHANNEL,                            /* q0 (lossy sums only) */
+  PPVM_OP_CORRELATED_LOSS_CHANNEL,                       /* q0, q1, p[0..2] (lossy sums) */
   PPVM_OP_COUNT_
 } ppvm_opcode;
 
@@ -74,6 +77,12 @@ typedef struct ppvm_op {
 #define PPVM_FLAG_EXACT_ORDER 2u     /* keep the reference's term order (IndexMap insertion
                                         order) through every op: disables fused rotation runs,
                                         which reorder terms (same terms, same coefficients) */
+#define PPVM_FLAG_LOSSY 4u           /* lossy words (LossyPauliWord): each qubit may also be lost
+                                        (L); at most 256 qubits.  Words of a lossy sum are passed
+                                        with 2*ceil(n/64) u64 per plane: the X plane's upper half
+                                        holds the loss bits (qubit q at bit q%64 of word
+                                        ceil(n/64) + q/64), the Z plane's upper half is zero, and a
+                                        lost qubit has x = z = 0 in the lower halves */
 
 /* ---- lifetime ------------------------------------------------------------------ */
 

@@ -80,29 +80,59 @@ inline uint64_t table_cap_for(size_t entries) {
 }
 
 // Word geometry and the strategy, shared by both map configurations.  A key is the X
-// plane's W words followed by the Z plane's W words.
+// plane's W words followed by the Z plane's W words; a lossy word (LossyPauliWord,
+// crates/ppvm-pauli-word/src/loss/data.rs:33-44) adds its loss plane's W words.  A lost qubit
+// (Pauli::L) has x = z = 0 and l = 1 (data.rs:218-230).
 struct Words {
   uint32_t n = 0;
   int W = 1;  // words per plane
   double thr = 1e-10;
   uint64_t maxw = UINT64_MAX;
+  uint64_t maxlw = UINT64_MAX;  // MaxLossWeight (strategy.rs:145-180)
   bool clifford_angles = false;
-  std::vector<uint64_t> preserve;  // flat [j][2W]
+  bool lossy = false;
+  std::vector<uint64_t> preserve;  // flat [j][kw()]
 
-  int kw() const { return 2 * W; }
-  size_t kb() const { return sizeof(uint64_t) * 2 * W; }
+  int kw() const { return (lossy ? 3 : 2) * W; }
+  size_t kb() const { return sizeof(uint64_t) * kw(); }
   bool get_x(const uint64_t* k, uint32_t q) const { return (k[q >> 6] >> (q & 63)) & 1u; }
   bool get_z(const uint64_t* k, uint32_t q) const { return (k[W + (q >> 6)] >> (q & 63)) & 1u; }
+  bool get_l(const uint64_t* k, uint32_t q) const {
+    return lossy && ((k[2 * W + (q >> 6)] >> (q & 63)) & 1u);
+  }
   static void set_bit(uint64_t* w, uint32_t q, bool b) {
     uint64_t m = 1ull << (q & 63);
     if (b) w[q >> 6] |= m; else w[q >> 6] &= ~m;
   }
   void set_x(uint64_t* k, uint32_t q, bool b) const { set_bit(k, q, b); }
   void set_z(uint64_t* k, uint32_t q, bool b) const { set_bit(k + W, q, b); }
+  void set_l(uint64_t* k, uint32_t q, bool b) const { set_bit(k + 2 * W, q, b); }
+  // Pauli::I/X/Z/Y/L on qubit q: the reference's `k.set(q, pauli)` (data.rs:255-283)
+  void set_code(uint64_t* k, uint32_t q, int code) const {  // 0 I, 1 X, 2 Z, 3 Y, 4 L
+    set_x(k, q, code == 1 || code == 3);
+    set_z(k, q, code == 2 || code == 3);
+    if (lossy) set_l(k, q, code == 4);
+  }
+  int code(const uint64_t* k, uint32_t q) const {
+    return get_l(k, q) ? 4 : ((int)get_x(k, q) | ((int)get_z(k, q) << 1));
+  }
+  // weight counts lost qubits too; loss_weight only those (loss/data.rs:132-200)
   uint64_t weight(const uint64_t* k) const {
     uint64_t t = 0;
-    for (int w = 0; w < W; ++w) t += __builtin_popcountll(k[w] | k[W + w]);
+    for (int w = 0; w < W; ++w) t += __builtin_popcountll(k[w] | k[W + w] | (lossy ? k[2 * W + w] : 0));
     return t;
+  }
+  uint64_t loss_weight(const uint64_t* k) const {
+    uint64_t t = 0;
+    if (lossy)
+      for (int w = 0; w < W; ++w) t += __builtin_popcountll(k[2 * W + w]);
+    return t;
+  }
+  // "Z?*" matches only words with no X bit and no lost qubit
+  bool zero_overlap_word(const uint64_t* k) const {
+    for (int w = 0; w < W; ++w)
+      if (k[w] | (lossy ? k[2 * W + w] : 0)) return false;
+    return true;
   }
 };
 
@@ -122,8 +152,8 @@ struct IndexStore : Words {
 
   void init() { rebuild_index(); }
   size_t len() const { return vals.size(); }
-  const uint64_t* key(size_t i) const { return &keys[i * 2 * W]; }
-  uint64_t* key(size_t i) { return &keys[i * 2 * W]; }
+  const uint64_t* key(size_t i) const { return &keys[i * kw()]; }
+  uint64_t* key(size_t i) { return &keys[i * kw()]; }
 
   void reserve_index(size_t expected) {  // empty table sized for `expected` entries
     uint64_t cap = table_cap_for(expected);
@@ -253,13 +283,67 @@ struct IndexStore : Words {
   }
   double overlap_with_zero() const {  // trace("Z?*"): fold in order over X-free words
     double acc = 0.0;
-    for (size_t i = 0; i < len(); ++i) {
-      const uint64_t* k = key(i);
-      bool xfree = true;
-      for (int w = 0; w < W; ++w) xfree &= (k[w] == 0);
-      if (xfree) acc += vals[i];
-    }
+    for (size_t i = 0; i < len(); ++i)
+      if (zero_overlap_word(key(i))) acc += vals[i];
     return acc;
+  }
+  // map_insert_multiple (data.rs:227-248): aux cleared; every parent's children `+=`-inserted
+  // into aux in iteration order (hashmap.rs:181-194); then consume (data.rs:180-189): the
+  // larger map takes the smaller one's entries with `+=` (hashmap.rs:302-308), in the smaller
+  // one's order, and ends up as the data map.  f(key, &v, out_keys, out_vals) appends children.
+  template <class F>
+  void map_insert_multiple(F f) {
+    aux_keys.clear();
+    aux_vals.clear();
+    std::vector<uint32_t> atab(table_cap_for(len()), kEmpty);
+    uint64_t amask = atab.size() - 1;
+    auto aux_find = [&](const uint64_t* k) -> long {
+      uint64_t s = fx_hash(k, kw()) & amask;
+      while (atab[s] != kEmpty) {
+        if (std::memcmp(&aux_keys[(size_t)atab[s] * kw()], k, kb()) == 0) return atab[s];
+        s = (s + 1) & amask;
+      }
+      return -1;
+    };
+    auto aux_add = [&](const uint64_t* k, double v) {
+      long j = aux_find(k);
+      if (j >= 0) {
+        aux_vals[j] += v;
+        return;
+      }
+      aux_keys.insert(aux_keys.end(), k, k + kw());
+      aux_vals.push_back(v);
+      if (2 * aux_vals.size() + 2 > atab.size()) {
+        atab.assign(table_cap_for(aux_vals.size()), kEmpty);
+        amask = atab.size() - 1;
+        for (size_t i = 0; i < aux_vals.size(); ++i) {
+          uint64_t s = fx_hash(&aux_keys[i * kw()], kw()) & amask;
+          while (atab[s] != kEmpty) s = (s + 1) & amask;
+          atab[s] = (uint32_t)i;
+        }
+        return;
+      }
+      uint64_t s = fx_hash(k, kw()) & amask;
+      while (atab[s] != kEmpty) s = (s + 1) & amask;
+      atab[s] = (uint32_t)(aux_vals.size() - 1);
+    };
+    std::vector<uint64_t> ck;
+    std::vector<double> cv;
+    for (size_t i = 0; i < len(); ++i) {
+      ck.clear();
+      cv.clear();
+      f(key(i), vals[i], ck, cv);
+      for (size_t j = 0; j < cv.size(); ++j) aux_add(&ck[j * kw()], cv[j]);
+    }
+    if (aux_vals.size() > len()) {  // aux.consume(data); swap
+      for (size_t i = 0; i < len(); ++i) aux_add(key(i), vals[i]);
+      keys.swap(aux_keys);
+      vals.swap(aux_vals);
+      rebuild_index();
+    } else {  // data.consume(aux)
+      const size_t na = aux_vals.size();
+      for (size_t j = 0; j < na; ++j) add_assign(&aux_keys[j * kw()], aux_vals[j]);
+    }
   }
 };
 
@@ -536,12 +620,8 @@ struct ShardStore : Words {
     pool->parallel_for(S, [&](long s) {
       const Shard& sh = data[s];
       double acc = 0.0;
-      for (size_t i = 0; i < sh.vals.size(); ++i) {
-        const uint64_t* k = &sh.keys[i * kw()];
-        bool xfree = true;
-        for (int w = 0; w < W; ++w) xfree &= (k[w] == 0);
-        if (xfree) acc += sh.vals[i];
-      }
+      for (size_t i = 0; i < sh.vals.size(); ++i)
+        if (zero_overlap_word(&sh.keys[i * kw()])) acc += sh.vals[i];
       part[s] = acc;
     });
     double acc = 0.0;
@@ -560,13 +640,16 @@ struct Sum : M {
   using M::set_z;
 
   // ---- Clifford gates (crates/ppvm-pauli-sum/src/sum/clifford.rs) ------------------
-  void g_x(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (get_z(k, q)) v *= -1.0; }); }
-  void g_y(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (get_x(k, q) ^ get_z(k, q)) v *= -1.0; }); }
-  void g_z(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (get_x(k, q)) v *= -1.0; }); }
+  // A gate on a lost qubit leaves the word alone (clifford.rs:42-199 check get_lbit first).
+  using M::get_l;
+  void g_x(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (!get_l(k, q) && get_z(k, q)) v *= -1.0; }); }
+  void g_y(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (!get_l(k, q) && (get_x(k, q) ^ get_z(k, q))) v *= -1.0; }); }
+  void g_z(uint32_t q) { this->scale([&](const uint64_t* k, double& v) { if (!get_l(k, q) && get_x(k, q)) v *= -1.0; }); }
   // single-qubit map_add gates: mode selects the bit map and the sign rule.
   enum Single { H, S, SDAG, SQX, SQXDAG, SQY, SQYDAG };
   void g_single(Single g, uint32_t q) {
     this->map_add([&](uint64_t* k, double& v) {
+      if (get_l(k, q)) return;
       bool x = get_x(k, q), z = get_z(k, q);
       bool neg = false;
       switch (g) {
@@ -585,6 +668,7 @@ struct Sum : M {
   enum Two { CNOT, CZ, CY };
   void g_two(Two g, uint32_t c, uint32_t t) {
     this->map_add([&](uint64_t* k, double& v) {
+      if (get_l(k, c) || get_l(k, t)) return;  // phase/clifford.rs:77,92,168
       bool xc = get_x(k, c), zc = get_z(k, c), xt = get_x(k, t), zt = get_z(k, t);
       bool neg = false;
       switch (g) {
@@ -609,7 +693,7 @@ struct Sum : M {
   // Each closure mirrors the reference fast path: parent *= cos; child = v * (eps * sin).
   void r_x(uint32_t q, double s, double co) {
     this->map_insert([&](uint64_t* k, double& v, double& cv) {
-      if (!get_z(k, q)) return false;
+      if (get_l(k, q) || !get_z(k, q)) return false;  // rot1.rs:60
       bool xb = get_x(k, q);
       double coeff = v;
       v *= co;
@@ -621,6 +705,7 @@ struct Sum : M {
   }
   void r_y(uint32_t q, double s, double co) {
     this->map_insert([&](uint64_t* k, double& v, double& cv) {
+      if (get_l(k, q)) return false;  // rot1.rs:85
       bool xb = get_x(k, q), zb = get_z(k, q);
       if (xb == zb) return false;
       double coeff = v;
@@ -633,6 +718,7 @@ struct Sum : M {
   }
   void r_z(uint32_t q, double s, double co) {
     this->map_insert([&](uint64_t* k, double& v, double& cv) {
+      if (get_l(k, q)) return false;  // rot1.rs:111
       bool xb = get_x(k, q);
       if (!xb) return false;
       bool zb = get_z(k, q);
@@ -644,8 +730,28 @@ struct Sum : M {
       return true;
     });
   }
+  // rotate_1 closure (rot1.rs:9-42) on qubit q about axis (ax, az): the loss fallback of the
+  // two-qubit rotations (rot2.rs:28-33, 70-75, 109-114, 149-154).  Levi-Civita sign of the
+  // axis times the qubit's Pauli, as rot_sign computes it for a one-qubit generator.
+  bool rot1_closure(uint64_t* k, double& v, double& cv, uint32_t q, bool ax, bool az, double s, double co) const {
+    if (get_l(k, q)) return false;
+    const bool x = get_x(k, q), z = get_z(k, q);
+    if (!((x & az) ^ (z & ax))) return false;
+    std::vector<uint64_t> gx(W, 0), gz(W, 0);
+    if (ax) gx[q >> 6] |= 1ull << (q & 63);
+    if (az) gz[q >> 6] |= 1ull << (q & 63);
+    const double eps = (double)rot_sign(gx.data(), gz.data(), k);
+    double coeff = v;
+    v *= co;
+    set_x(k, q, x ^ ax);
+    set_z(k, q, z ^ az);
+    cv = coeff * (eps * s);
+    return true;
+  }
   void r_zz(uint32_t a, uint32_t b, double s, double co) {
     this->map_insert([&](uint64_t* k, double& v, double& cv) {
+      if (get_l(k, a)) return rot1_closure(k, v, cv, b, false, true, s, co);
+      if (get_l(k, b)) return rot1_closure(k, v, cv, a, false, true, s, co);
       bool xa = get_x(k, a), xb = get_x(k, b);
       if (xa == xb) return false;
       bool za = get_z(k, a), zb = get_z(k, b);
@@ -660,6 +766,8 @@ struct Sum : M {
   }
   void r_xx(uint32_t a, uint32_t b, double s, double co) {
     this->map_insert([&](uint64_t* k, double& v, double& cv) {
+      if (get_l(k, a)) return rot1_closure(k, v, cv, b, true, false, s, co);
+      if (get_l(k, b)) return rot1_closure(k, v, cv, a, true, false, s, co);
       bool za = get_z(k, a), zb = get_z(k, b);
       if (za == zb) return false;
       bool xa = get_x(k, a), xb = get_x(k, b);
@@ -674,6 +782,8 @@ struct Sum : M {
   }
   void r_yy(uint32_t a, uint32_t b, double s, double co) {
     this->map_insert([&](uint64_t* k, double& v, double& cv) {
+      if (get_l(k, a)) return rot1_closure(k, v, cv, b, true, true, s, co);
+      if (get_l(k, b)) return rot1_closure(k, v, cv, a, true, true, s, co);
       bool xa = get_x(k, a), za = get_z(k, a), xb = get_x(k, b), zb = get_z(k, b);
       bool pa = xa ^ za, pb = xb ^ zb;
       if (pa == pb) return false;
@@ -710,14 +820,19 @@ struct Sum : M {
       par ^= __builtin_parityll((k[w] & gz[w]) ^ (k[W + w] & gx[w]));
     return par;
   }
-  // Generic exp(-i theta/2 G): rotate_1 / rotate_2 generalised to any support.
+  // Generic exp(-i theta/2 G): rotate_1 / rotate_2 generalised to any support.  On a lossy
+  // word the generator acts only on qubits that are not lost, which is the reference's loss
+  // fallback of rotate_2 (rot2.rs:26-33) extended to any support.
   void r_pauli(const uint64_t* gx, const uint64_t* gz, double s, double co) {
     this->map_insert([&](uint64_t* k, double& v, double& cv) {
-      if (!anticommutes(gx, gz, k)) return false;
-      double eps = (double)rot_sign(gx, gz, k);
+      std::vector<uint64_t> ex(gx, gx + W), ez(gz, gz + W);
+      if (this->lossy)
+        for (int w = 0; w < W; ++w) { ex[w] &= ~k[2 * W + w]; ez[w] &= ~k[2 * W + w]; }
+      if (!anticommutes(ex.data(), ez.data(), k)) return false;
+      double eps = (double)rot_sign(ex.data(), ez.data(), k);
       double coeff = v;
       v *= co;
-      for (int w = 0; w < W; ++w) { k[w] ^= gx[w]; k[W + w] ^= gz[w]; }
+      for (int w = 0; w < W; ++w) { k[w] ^= ex[w]; k[W + w] ^= ez[w]; }
       cv = coeff * (eps * s);
       return true;
     });
@@ -727,9 +842,12 @@ struct Sum : M {
   // Clifford compositions (e.g. RZZ(-pi/2) == CZ, S_DAG, S_DAG).
   void r_pauli_clifford(const uint64_t* gx, const uint64_t* gz, double sin_sign) {
     this->map_add([&](uint64_t* k, double& v) {
-      if (!anticommutes(gx, gz, k)) return;
-      double eps = (double)rot_sign(gx, gz, k);
-      for (int w = 0; w < W; ++w) { k[w] ^= gx[w]; k[W + w] ^= gz[w]; }
+      std::vector<uint64_t> ex(gx, gx + W), ez(gz, gz + W);
+      if (this->lossy)
+        for (int w = 0; w < W; ++w) { ex[w] &= ~k[2 * W + w]; ez[w] &= ~k[2 * W + w]; }
+      if (!anticommutes(ex.data(), ez.data(), k)) return;
+      double eps = (double)rot_sign(ex.data(), ez.data(), k);
+      for (int w = 0; w < W; ++w) { k[w] ^= ex[w]; k[W + w] ^= ez[w]; }
       v = v * (eps * sin_sign);
     });
   }
@@ -741,17 +859,19 @@ struct Sum : M {
     double zf = one - p[0] * 2.0 - p[1] * 2.0;
     double yf = one - p[0] * 2.0 - p[2] * 2.0;
     this->scale([&](const uint64_t* k, double& v) {
+      if (get_l(k, q)) return;  // noise.rs:25
       int code = (int)get_x(k, q) | ((int)get_z(k, q) << 1);
       if (code == 1) v *= xf; else if (code == 2) v *= zf; else if (code == 3) v *= yf;
     });
   }
   void depolarize1(uint32_t q, double p) {  // noise.rs:107-116
     double f = 1.0 - p * (4.0 / 3.0);
-    this->scale([&](const uint64_t* k, double& v) { if (get_x(k, q) | get_z(k, q)) v *= f; });
+    this->scale([&](const uint64_t* k, double& v) { if (!get_l(k, q) && (get_x(k, q) | get_z(k, q))) v *= f; });
   }
   void depolarize2(uint32_t a, uint32_t b, double p) {  // noise.rs:119-129
     double f = 1.0 - p * (16.0 / 15.0);
     this->scale([&](const uint64_t* k, double& v) {
+      if (get_l(k, a) || get_l(k, b)) return;  // noise.rs:122
       if (get_x(k, a) | get_z(k, a) | get_x(k, b) | get_z(k, b)) v *= f;
     });
   }
@@ -779,6 +899,7 @@ struct Sum : M {
         f[ca][cb] = acc;
       }
     this->scale([&](const uint64_t* k, double& v) {
+      if (get_l(k, a) || get_l(k, b)) return;  // a lost qubit: no channel (noise.rs:98-102)
       const int ca = (int)get_x(k, a) | ((int)get_z(k, a) << 1);
       const int cb = (int)get_x(k, b) | ((int)get_z(k, b) << 1);
       if (ca | cb) v *= f[ca][cb];
@@ -790,6 +911,7 @@ struct Sum : M {
     const double om = 1.0 - gamma;
     const double sxy = std::sqrt(om);
     this->map_insert([&](uint64_t* ck, double& v, double& cv) {
+      if (get_l(ck, q)) return false;  // noise.rs:138 (L like I)
       if (get_x(ck, q)) {
         v *= sxy;
         return false;
@@ -802,6 +924,69 @@ struct Sum : M {
     });
   }
 
+  // ---- loss channels (crates/ppvm-pauli-sum/src/sum/noise.rs:165-275) -----------------
+  // loss_channel (noise.rs:165-181): L on q -> child with I on q, v * p (parent unchanged);
+  // I, X, Y, Z on q: v *= 1 - p.
+  void loss_channel(uint32_t q, double p) {
+    this->map_insert([&](uint64_t* ck, double& v, double& cv) {
+      if (this->code(ck, q) == 4) {
+        cv = v * p;
+        this->set_code(ck, q, 0);
+        return true;
+      }
+      v *= 1.0 - p;
+      return false;
+    });
+  }
+  // correlated_loss_channel (noise.rs:184-243) through map_insert_multiple.
+  void correlated_loss_channel(uint32_t a, uint32_t b, const double p[3]) {
+    const int kw = this->kw();
+    this->map_insert_multiple([&](const uint64_t* k, double& v, std::vector<uint64_t>& ok,
+                                  std::vector<double>& ov) {
+      const int ca = this->code(k, a), cb = this->code(k, b);
+      auto child = [&](int na, int nb, double val) {
+        const size_t o = ok.size();
+        ok.insert(ok.end(), k, k + kw);
+        this->set_code(&ok[o], a, na);
+        this->set_code(&ok[o], b, nb);
+        ov.push_back(val);
+      };
+      if (ca == 4 && cb == 4) {  // both lost: (I,L), (L,I) with p[2]; (I,I) with p[0]
+        const double v_il = v * p[2];
+        child(0, 4, v_il);
+        child(4, 0, v_il);
+        child(0, 0, v * p[0]);
+      } else if (cb == 4) {  // qubit 1 lost
+        const double nv = v * p[1];
+        v *= 1.0 - p[2];
+        child(ca, 0, nv);
+      } else if (ca == 4) {  // qubit 0 lost
+        const double nv = v * p[1];
+        v *= 1.0 - p[2];
+        child(0, cb, nv);
+      } else {
+        v *= 1.0 - p[1] * 2.0 - p[0];
+      }
+    });
+  }
+  // reset_loss_channel (noise.rs:245-275): L on q -> v *= 0.0; I or Z -> child with L on q
+  // (same coefficient); X, Y unchanged.
+  void reset_loss_channel(uint32_t q) {
+    this->map_insert([&](uint64_t* ck, double& v, double& cv) {
+      const int c = this->code(ck, q);
+      if (c == 4) {
+        v *= 0.0;
+        return false;
+      }
+      if (c == 0 || c == 2) {
+        cv = v;
+        this->set_code(ck, q, 4);
+        return true;
+      }
+      return false;
+    });
+  }
+
   // ---- truncation (data.rs:275-311, strategy.rs) -------------------------------------
   void strategy() {
     double t = this->thr;
@@ -810,24 +995,30 @@ struct Sum : M {
       uint64_t mw = this->maxw;
       this->retain([&](const uint64_t* k, double) { return this->weight(k) <= mw; });
     }
+    if (this->lossy && this->maxlw != UINT64_MAX) {  // MaxLossWeight (strategy.rs:165-180)
+      uint64_t ml = this->maxlw;
+      this->retain([&](const uint64_t* k, double) { return this->loss_weight(k) <= ml; });
+    }
   }
   bool is_preserved(const uint64_t* k) const {
-    size_t np = this->preserve.size() / (2 * W);
+    const int kw = this->kw();
+    size_t np = this->preserve.size() / kw;
     for (size_t j = 0; j < np; ++j)
-      if (std::memcmp(&this->preserve[j * 2 * W], k, this->kb()) == 0) return true;
+      if (std::memcmp(&this->preserve[j * kw], k, this->kb()) == 0) return true;
     return false;
   }
   void truncate() {
     if (this->preserve.empty()) { strategy(); return; }
+    const int kw = this->kw();
     std::vector<uint64_t> sk;
     std::vector<double> sv;
     this->for_each([&](const uint64_t* k, double v) {
-      if (is_preserved(k)) { sk.insert(sk.end(), k, k + 2 * W); sv.push_back(v); }
+      if (is_preserved(k)) { sk.insert(sk.end(), k, k + kw); sv.push_back(v); }
     });
     strategy();
     double dummy;
     for (size_t j = 0; j < sv.size(); ++j)
-      if (!this->get(&sk[j * 2 * W], dummy)) this->add_assign(&sk[j * 2 * W], sv[j]);
+      if (!this->get(&sk[j * kw], dummy)) this->add_assign(&sk[j * kw], sv[j]);
   }
 };
 
@@ -888,8 +1079,8 @@ Pattern parse_pattern(const char* s) {  // parse.rs:32-127
 // contains.rs:120-151 (match_position :44-66, match_star :68-84, match_repeat :86-116)
 bool pattern_contains(const Pattern& P, const Words& S, const uint64_t* k) {
   uint32_t pos = 0, n = S.n;
-  auto code = [&](uint32_t q) { return (unsigned)S.get_x(k, q) | ((unsigned)S.get_z(k, q) << 1); };
-  auto accepts = [](unsigned acc, unsigned c) { return (acc >> (c == 0 ? 0 : c == 1 ? 1 : c == 2 ? 2 : 3)) & 1u; };
+  auto code = [&](uint32_t q) { return (unsigned)S.code(k, q); };  // 4 = L: no item accepts it
+  auto accepts = [](unsigned acc, unsigned c) { return c < 4 && ((acc >> c) & 1u); };
   for (const PatItem& it : P.items) {
     if (it.kind == 0) {
       bool next = false;
@@ -983,6 +1174,19 @@ int run_op(Sum<M>* s, const ppvm_op& op) {
     case PPVM_OP_DEPOLARIZE2: if (!two_ok()) return 1; s->depolarize2(op.q0, op.q1, op.theta); return 0;
     case PPVM_OP_TRUNCATE: s->truncate(); return 0;
     case PPVM_OP_AMPLITUDE_DAMPING: if (!qok(s, op.q0)) return 1; s->amplitude_damping(op.q0, op.theta); return 0;
+    case PPVM_OP_LOSS_CHANNEL: if (!qok(s, op.q0)) return 1; s->loss_channel(op.q0, op.theta); return 0;
+    case PPVM_OP_RESET_LOSS_CHANNEL:  // defined for lossy words only (noise.rs:245-252)
+      if (!qok(s, op.q0) || !s->lossy) return 1;
+      s->reset_loss_channel(op.q0);
+      return 0;
+    case PPVM_OP_CORRELATED_LOSS_CHANNEL:
+      if (!two_ok()) return 1;
+      // The DashMap configuration inserts a parent's children with a plain `insert`
+      // from several threads at once (crates/ppvm-traits/src/map/dashmap.rs:168-183): the
+      // value of a key with several children depends on thread timing, so it is not restated.
+      if constexpr (std::is_same<M, ShardStore>::value) return 1;
+      else s->correlated_loss_channel(op.q0, op.q1, op.p);
+      return 0;
     default: return 1;
   }
 }
@@ -1035,6 +1239,7 @@ Handle* make_handle(uint32_t n, double thr, uint64_t maxw, uint32_t flags, int t
   s.thr = thr;
   s.maxw = maxw;
   s.clifford_angles = (flags & PPVM_FLAG_CLIFFORD_ANGLES) != 0;
+  s.lossy = (flags & PPVM_FLAG_LOSSY) != 0;
   if constexpr (std::is_same<M, ShardStore>::value) s.threads = threads;
   s.init();
   return h;
@@ -1044,8 +1249,30 @@ Handle* make_handle(uint32_t n, double thr, uint64_t maxw, uint32_t flags, int t
 
 extern "C" {
 
+// Words cross this interface in the engine's layout: W = ceil(n/64) words per plane, or for
+// a lossy sum 2W, the X plane's upper W words holding the loss bits and the Z plane's upper W
+// words zero (include/ppvm_cuda.h, PPVM_FLAG_LOSSY).  These convert to and from a key.
+static int api_words(const Words& s) { return s.lossy ? 2 * s.W : s.W; }
+static void key_from_api(const Words& s, const uint64_t* x, const uint64_t* z, uint64_t* key) {
+  for (int w = 0; w < s.W; ++w) {
+    key[w] = x[w];
+    key[s.W + w] = z[w];
+    if (s.lossy) key[2 * s.W + w] = x[s.W + w];
+  }
+}
+static void key_to_api(const Words& s, const uint64_t* key, uint64_t* x, uint64_t* z) {
+  for (int w = 0; w < s.W; ++w) {
+    x[w] = key[w];
+    z[w] = key[s.W + w];
+    if (s.lossy) {
+      x[s.W + w] = key[2 * s.W + w];
+      z[s.W + w] = 0;
+    }
+  }
+}
+
 void* oracle_create(uint32_t n, double thr, uint64_t maxw, uint32_t flags) {
-  if (n == 0) return nullptr;
+  if (n == 0 || ((flags & PPVM_FLAG_LOSSY) && n > 256)) return nullptr;
   return make_handle<IndexStore>(n, thr, maxw, flags, 1);
 }
 // The DashMap configuration on `threads` threads (0: every hardware thread).
@@ -1056,16 +1283,19 @@ void* oracle_create_sharded(uint32_t n, double thr, uint64_t maxw, uint32_t flag
 }
 void oracle_destroy(void* h) { delete (Handle*)h; }
 void* oracle_clone(void* h) { return ((Handle*)h)->clone(); }
-int oracle_words(void* h) { return ((Handle*)h)->words().W; }
+int oracle_words(void* h) { return api_words(((Handle*)h)->words()); }
+// MaxLossWeight of a lossy sum's strategy (UINT64_MAX: off).
+void oracle_set_max_loss_weight(void* h, uint64_t maxlw) { ((Handle*)h)->words().maxlw = maxlw; }
 size_t oracle_len(void* h) { return ((Handle*)h)->len(); }
 
 // x, z term-major [k][W]
 int oracle_add_terms(void* h, const uint64_t* x, const uint64_t* z, const double* c, size_t k) {
   Handle* s = (Handle*)h;
-  const int W = s->words().W;
-  std::vector<uint64_t> key(2 * W);
+  const Words& ws = s->words();
+  const int A = api_words(ws);
+  std::vector<uint64_t> key(ws.kw());
   for (size_t i = 0; i < k; ++i) {
-    for (int w = 0; w < W; ++w) { key[w] = x[i * W + w]; key[W + w] = z[i * W + w]; }
+    key_from_api(ws, x + i * A, z + i * A, key.data());
     s->add_assign(key.data(), c[i]);
   }
   return 0;
@@ -1084,11 +1314,9 @@ int oracle_two_qubit_pauli_error(void* h, const uint32_t* pairs, size_t k_flat, 
 }
 int oracle_set_preserve(void* h, const uint64_t* x, const uint64_t* z, size_t k) {
   Words& s = ((Handle*)h)->words();
-  s.preserve.clear();
-  for (size_t i = 0; i < k; ++i) {
-    for (int w = 0; w < s.W; ++w) s.preserve.push_back(x[i * s.W + w]);
-    for (int w = 0; w < s.W; ++w) s.preserve.push_back(z[i * s.W + w]);
-  }
+  const int A = api_words(s);
+  s.preserve.assign(k * s.kw(), 0);
+  for (size_t i = 0; i < k; ++i) key_from_api(s, x + i * A, z + i * A, &s.preserve[i * s.kw()]);
   return 0;
 }
 // Runs ops in order; records the live count entering each op into counts (may be NULL).
@@ -1130,11 +1358,12 @@ double oracle_overlap(void* a, void* b) {
 }
 size_t oracle_export(void* h, uint64_t* x, uint64_t* z, double* c, size_t cap) {
   Handle* s = (Handle*)h;
-  const int W = s->words().W;
+  const Words& ws = s->words();
+  const int A = api_words(ws);
   size_t i = 0;
   s->each([&](const uint64_t* k, double v) {
     if (i >= cap) return;
-    for (int w = 0; w < W; ++w) { x[i * W + w] = k[w]; z[i * W + w] = k[W + w]; }
+    key_to_api(ws, k, x + i * A, z + i * A);
     c[i] = v;
     ++i;
   });

@@ -56,6 +56,7 @@ def lib():
         L.oracle_clone.argtypes = [vp]
         L.oracle_words.restype = ctypes.c_int
         L.oracle_words.argtypes = [vp]
+        L.oracle_set_max_loss_weight.argtypes = [vp, u64]
         L.oracle_len.restype = sz
         L.oracle_len.argtypes = [vp]
         L.oracle_add_terms.argtypes = [vp, P64, P64, PD, sz]
@@ -104,14 +105,18 @@ class OracleSum:
     By default the IndexMap configuration (insertion-ordered map, one thread), the one every
     parity test compares against.  ``threads`` selects the reference's DashMap configuration
     instead, on that many host threads (0: all): the same terms and coefficients, in
-    per-shard order."""
+    per-shard order.  ``lossy`` holds LossyPauliWord terms; their words cross this interface
+    in the engine's lossy layout (2 * ceil(n/64) words per plane, loss bits in the X plane's
+    upper half), and ``max_loss_weight`` is the strategy's MaxLossWeight."""
 
     def __init__(self, n_qubits: int, min_abs_coeff: float = 1e-10,
-                 max_weight: int | None = None, clifford_angles: bool = False, threads: int | None = None):
+                 max_weight: int | None = None, clifford_angles: bool = False, threads: int | None = None,
+                 lossy: bool = False, max_loss_weight: int | None = None):
         L = lib()
         self.n = n_qubits
+        self.lossy = bool(lossy)
         mw = (1 << 64) - 1 if max_weight is None else int(max_weight)
-        flags = 1 if clifford_angles else 0
+        flags = (1 if clifford_angles else 0) | (4 if lossy else 0)
         if threads is None:
             self._h = L.oracle_create(n_qubits, min_abs_coeff, mw, flags)
         else:
@@ -119,6 +124,8 @@ class OracleSum:
         if not self._h:
             raise ValueError("oracle_create failed")
         self.W = L.oracle_words(self._h)
+        if max_loss_weight is not None:
+            L.oracle_set_max_loss_weight(self._h, int(max_loss_weight))
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -128,7 +135,7 @@ class OracleSum:
 
     def clone(self) -> "OracleSum":
         o = OracleSum.__new__(OracleSum)
-        o.n, o.W = self.n, self.W
+        o.n, o.W, o.lossy = self.n, self.W, self.lossy
         o._h = lib().oracle_clone(self._h)
         return o
 

@@ -21,13 +21,15 @@ RXX, RYY, RZZ = 16, 17, 18
 PAULI_ERROR, DEPOLARIZE1, DEPOLARIZE2 = 19, 20, 21
 TRUNCATE = 22
 AMPLITUDE_DAMPING = 23
+LOSS_CHANNEL, RESET_LOSS_CHANNEL, CORRELATED_LOSS_CHANNEL = 24, 25, 26
 
 NAMES = {
     X: "x", Y: "y", Z: "z", H: "h", S: "s", S_DAG: "s_dag", SQRT_X: "sqrt_x",
     SQRT_X_DAG: "sqrt_x_dag", SQRT_Y: "sqrt_y", SQRT_Y_DAG: "sqrt_y_dag", CNOT: "cnot",
     CZ: "cz", CY: "cy", RX: "rx", RY: "ry", RZ: "rz", RXX: "rxx", RYY: "ryy", RZZ: "rzz",
     PAULI_ERROR: "pauli_error", DEPOLARIZE1: "depolarize1", DEPOLARIZE2: "depolarize2",
-    TRUNCATE: "truncate", AMPLITUDE_DAMPING: "amplitude_damping",
+    TRUNCATE: "truncate", AMPLITUDE_DAMPING: "amplitude_damping", LOSS_CHANNEL: "loss_channel",
+    RESET_LOSS_CHANNEL: "reset_loss_channel", CORRELATED_LOSS_CHANNEL: "correlated_loss_channel",
 }
 SINGLE_CLIFFORD = {X, Y, Z, H, S, S_DAG, SQRT_X, SQRT_X_DAG, SQRT_Y, SQRT_Y_DAG}
 TWO_CLIFFORD = {CNOT, CZ, CY}
@@ -70,6 +72,18 @@ def amplitude_damping(q: int, gamma: float):
     return (AMPLITUDE_DAMPING, q, 0, float(gamma), _ZERO3)
 
 
+def loss_channel(q: int, p: float):
+    return (LOSS_CHANNEL, q, 0, float(p), _ZERO3)
+
+
+def reset_loss_channel(q: int):
+    return (RESET_LOSS_CHANNEL, q, 0, 0.0, _ZERO3)
+
+
+def correlated_loss_channel(a: int, b: int, p):
+    return (CORRELATED_LOSS_CHANNEL, a, b, 0.0, tuple(float(v) for v in p))
+
+
 def truncate():
     return (TRUNCATE, 0, 0, 0.0, _ZERO3)
 
@@ -100,6 +114,39 @@ def parse_word(s: str, n_qubits: int | None = None):
         elif c != "I":
             raise ValueError(f"Invalid Pauli character: {c}")
     return x, z
+
+
+def lossy_words(n_qubits: int) -> int:
+    """Words per plane of a lossy sum: the X plane's upper half holds the loss bits."""
+    return 2 * words(n_qubits)
+
+
+def parse_lossy_word(s: str, n_qubits: int | None = None):
+    """Lossy Pauli string (I, X, Y, Z, L) -> (x[2W], z[2W]) in the lossy layout: loss bit of
+    qubit q at bit q % 64 of X word W + q // 64 (crates/ppvm-pauli-word/src/loss/data.rs:318-377
+    parses the same alphabet; '_' is skipped)."""
+    chars = [c for c in s if c != "_"]
+    n = len(chars) if n_qubits is None else n_qubits
+    if len(chars) != n:
+        raise ValueError(f"word {s!r} has {len(chars)} qubits, expected {n}")
+    W = words(n)
+    x = np.zeros(2 * W, dtype=np.uint64)
+    z = np.zeros(2 * W, dtype=np.uint64)
+    plain = "".join("I" if c == "L" else c for c in chars)
+    x[:W], z[:W] = parse_word(plain, n)
+    for q, c in enumerate(chars):
+        if c == "L":
+            x[W + q // 64] |= np.uint64(1) << np.uint64(q % 64)
+    return x, z
+
+
+def lossy_word_str(x, z, n_qubits: int) -> str:
+    W = words(n_qubits)
+    out = list(word_str(x[:W], z[:W], n_qubits))
+    for q in range(n_qubits):
+        if (int(x[W + q // 64]) >> (q % 64)) & 1:
+            out[q] = "L"
+    return "".join(out)
 
 
 def word_str(x, z, n_qubits: int) -> str:
