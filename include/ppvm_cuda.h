@@ -82,7 +82,10 @@ typedef struct ppvm_op {
                                         with 2*ceil(n/64) u64 per plane: the X plane's upper half
                                         holds the loss bits (qubit q at bit q%64 of word
                                         ceil(n/64) + q/64), the Z plane's upper half is zero, and a
-                                        lost qubit has x = z = 0 in the lower halves */
+                                        lost qubit has x = z = 0 in the lower halves.  A lossy sum
+                                        keeps the reference's term order through every op (as
+                                        with PPVM_FLAG_EXACT_ORDER): the correlated loss channel
+                                        adds up to three children per key in that order */
 
 /* ---- lifetime ------------------------------------------------------------------ */
 
@@ -167,6 +170,23 @@ ppvm_status ppvm_pauli_error(ppvm_sum* sum, const uint32_t* targets, size_t k, c
 ppvm_status ppvm_depolarize1(ppvm_sum* sum, const uint32_t* targets, size_t k, double p, int truncate);
 ppvm_status ppvm_depolarize2(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat, double p,
                              int truncate);
+/* Lossy sums (PPVM_FLAG_LOSSY) only; PPVM_EINVAL on a plain sum.
+ * LossChannel::loss_channel (crates/ppvm-pauli-sum/src/sum/noise.rs:165-181; Python binding
+ * crates/ppvm-python-native/src/interface.rs:18-24) on each target: L -> keeps, plus I with p;
+ * I, X, Y, Z -> (1 - p). */
+ppvm_status ppvm_loss_channel(ppvm_sum* sum, const uint32_t* targets, size_t k, double p, int truncate);
+/* ResetLossChannel::reset_loss_channel (noise.rs:245-275; interface.rs:40-46) on each target:
+ * L -> 0; I, Z -> keeps, plus L with the same coefficient; X, Y unchanged. */
+ppvm_status ppvm_reset_loss_channel(ppvm_sum* sum, const uint32_t* targets, size_t k, int truncate);
+/* CorrelatedLossChannel::correlated_loss_channel (noise.rs:184-243; interface.rs:26-38) on each
+ * pair (a, b) of pairs_flat (even length, else PPVM_EINVAL), p = {p0, p1, p2} as the reference
+ * documents them (both lost together, one lost, the second lost after the first). */
+ppvm_status ppvm_correlated_loss_channel(ppvm_sum* sum, const uint32_t* pairs_flat, size_t k_flat,
+                                         const double p[3], int truncate);
+/* MaxLossWeight (crates/ppvm-pauli-sum/src/strategy.rs:145-180) of a lossy sum's strategy, run
+ * after the coefficient threshold and the weight cap, as the Python binding's lossy tiers
+ * combine them (interface.rs:58-66).  UINT64_MAX (the default) turns it off. */
+ppvm_status ppvm_sum_set_max_loss_weight(ppvm_sum* sum, uint64_t max_loss_weight);
 /* TwoQubitPauliError::two_qubit_pauli_error (noise.rs:39-105), applied pair by pair
  * (two_qubit_pauli_error_many, crates/ppvm-traits/src/traits/noise.rs:77-81).  p[0..15) are
  * the probabilities of IX IY IZ XI XX XY XZ YI YX YY YZ ZI ZX ZY ZZ, first letter on the

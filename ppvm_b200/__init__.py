@@ -6,14 +6,14 @@ reference) and drives the CUDA library ``libppvm_cuda.so`` through its C ABI
 loaded on first use and a missing or unloadable library raises immediately.
 """
 
-__all__ = ["PauliSum", "gates", "circuits"]
+__all__ = ["PauliSum", "LossyPauliSum", "gates", "circuits"]
 
 
 def __getattr__(name):
-    if name == "PauliSum":
-        from .paulisum import PauliSum
+    if name in ("PauliSum", "LossyPauliSum"):
+        from . import paulisum
 
-        return PauliSum
+        return getattr(paulisum, name)
     if name in ("gates", "circuits"):
         import importlib
 

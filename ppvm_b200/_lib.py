@@ -17,6 +17,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "ppvm_cuda.h")
 OK, EINVAL, ECAPACITY, ECUDA, ETIMEOUT, ENODEV = range(6)
 FLAG_CLIFFORD_ANGLES = 1
 FLAG_EXACT_ORDER = 2
+FLAG_LOSSY = 4
 UMAX = (1 << 64) - 1
 
 
@@ -67,6 +68,10 @@ _SIGS = {
     "ppvm_pauli_error": [_P, _U32P, _SZ, _DP, _I],
     "ppvm_depolarize1": [_P, _U32P, _SZ, ctypes.c_double, _I],
     "ppvm_depolarize2": [_P, _U32P, _SZ, ctypes.c_double, _I],
+    "ppvm_loss_channel": [_P, _U32P, _SZ, ctypes.c_double, _I],
+    "ppvm_reset_loss_channel": [_P, _U32P, _SZ, _I],
+    "ppvm_correlated_loss_channel": [_P, _U32P, _SZ, ctypes.POINTER(ctypes.c_double), _I],
+    "ppvm_sum_set_max_loss_weight": [_P, ctypes.c_uint64],
     "ppvm_two_qubit_pauli_error": [_P, _U32P, _SZ, _DP, _I],
     "ppvm_amplitude_damping": [_P, ctypes.c_uint32, ctypes.c_double, _I],
     "ppvm_truncate": [_P],

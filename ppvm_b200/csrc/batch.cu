@@ -963,6 +963,9 @@ ppvm_status ppvm_batch_set_ops(ppvm_batch* b, size_t inst, const ppvm_op* ops, s
   for (size_t i = 0; i < n_ops; ++i) {
     const ppvm_op& op = ops[i];
     if (op.flags != 0 || op.code >= PPVM_OP_COUNT_) return bfail(PPVM_EINVAL, "bad op code or flags");
+    if (op.code == PPVM_OP_LOSS_CHANNEL || op.code == PPVM_OP_RESET_LOSS_CHANNEL ||
+        op.code == PPVM_OP_CORRELATED_LOSS_CHANNEL)
+      return bfail(PPVM_EINVAL, "batched instances hold plain words: loss channels need a lossy PauliSum");
     BOp bo;
     std::memset(&bo, 0, sizeof(bo));
     if (op.code == PPVM_OP_TRUNCATE) {

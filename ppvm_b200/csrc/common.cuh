@@ -70,10 +70,13 @@ struct Planes {
   unsigned long long cap;
 };
 
-// A Pauli generator (rotation axis) as X/Z plane masks.
+// A Pauli generator (rotation axis) as X/Z plane masks.  lw: for a lossy sum, the first loss
+// word of the X plane (the generator then acts only on qubits that are not lost); 0 otherwise.
 struct Gen {
   uint64_t gx[kMaxW];
   uint64_t gz[kMaxW];
+  uint32_t lw;
+  uint32_t reserved;
 };
 
 // ---- memory ordering helpers (decoupled look-back) ----------------------------------

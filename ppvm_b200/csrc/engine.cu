@@ -25,6 +25,7 @@
 #include "runs.cuh"
 #include "tableau.cuh"
 #include "budget.cuh"
+#include "loss.cuh"
 #include "noise.cuh"
 
 using namespace ppvm;
@@ -93,12 +94,12 @@ struct ProfLaunch {
 
 enum Family {
   F_SCAN = 0, F_PAIR, F_APPLY, F_COMMIT, F_CLIFF, F_TRUNC, F_READ,
-  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_GROUPS, F_RUN_PLACE, F_TABLEAU, F_COUNT
+  F_RUN_CLASSIFY, F_RUN_ORDER, F_RUN_SCATTER, F_RUN_GROUPS, F_RUN_PLACE, F_TABLEAU, F_LOSS, F_COUNT
 };
 const char* kFamilyNames[F_COUNT] = {"rot_scan", "rot_pair", "rot_apply", "rot_commit",
                                      "clifford", "truncate", "readout",
                                      "run_classify", "run_order", "run_scatter", "run_groups", "run_place",
-                                     "tableau"};
+                                     "tableau", "loss"};
 
 // One pinned host chunk and its device twin: per-call uploads (op descriptors, run
 // descriptors, tableaux) are packed here and copied with truly asynchronous copies.
@@ -124,9 +125,12 @@ struct ppvm_sum {
   cudaStream_t stream = nullptr;
   bool own_stream = true;
   uint32_t n = 0;
-  int W = 1;
+  int W = 1;                   // words per plane (a lossy sum: 2 * wr, the loss bits in X's upper half)
+  int wr = 1;                  // words of the qubits' X/Z bits: ceil(n/64)
+  bool lossy = false;          // PPVM_FLAG_LOSSY
   double thr = 1e-10;
   uint64_t maxw = UINT64_MAX;
+  uint64_t maxlw = UINT64_MAX;  // MaxLossWeight of a lossy sum's strategy
   uint32_t flags = 0;
   unsigned long long cap = 0;
   unsigned long long n_host = 0;  // live count at the last synchronisation
@@ -345,6 +349,27 @@ ppvm_status ensure_device(int dev) {
   if (dev < 0 || dev >= count) return fail(PPVM_EINVAL, "device ordinal out of range");
   CUDA_TRY(cudaSetDevice(dev));
   if (g_sm_count == 0) CUDA_TRY(cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev));
+  return PPVM_OK;
+}
+
+// Words handed in by a caller: bits at or above n_qubits clear; on a lossy sum the Z plane's
+// upper words clear and a lost qubit without X or Z bits (it is L, not X, Y or Z).
+ppvm_status check_words(const ppvm_sum* s, const uint64_t* x, const uint64_t* z, size_t k) {
+  const int W = s->W, wr = s->wr;
+  const int tail = (int)(s->n % 64);
+  const uint64_t top = tail ? ~((1ull << tail) - 1) : 0ull;
+  for (size_t i = 0; i < k; ++i) {
+    const uint64_t* xi = x + i * W;
+    const uint64_t* zi = z + i * W;
+    if ((xi[wr - 1] | zi[wr - 1]) & top) return fail(PPVM_EINVAL, "word has bits set at or above n_qubits");
+    if (!s->lossy) continue;
+    if (xi[W - 1] & top) return fail(PPVM_EINVAL, "word has loss bits set at or above n_qubits");
+    for (int w = 0; w < wr; ++w) {
+      if (zi[wr + w]) return fail(PPVM_EINVAL, "a lossy word's Z plane has bits in its loss half");
+      if (xi[wr + w] & (xi[w] | zi[w]))
+        return fail(PPVM_EINVAL, "a lost qubit cannot also carry X or Z (LossyPauliWord::get panics)");
+    }
+  }
   return PPVM_OK;
 }
 
@@ -610,6 +635,7 @@ bool is_local(const ppvm_sum* s, const ppvm_op& op) {
     case PPVM_OP_RXX: case PPVM_OP_RYY: case PPVM_OP_RZZ:
       return is_clifford_angle(s, op.theta);
     case PPVM_OP_TRUNCATE: case PPVM_OP_AMPLITUDE_DAMPING: return false;
+    case PPVM_OP_LOSS_CHANNEL: case PPVM_OP_RESET_LOSS_CHANNEL: case PPVM_OP_CORRELATED_LOSS_CHANNEL: return false;
     case kOpPauliError2: return true;
     default: return op.code < PPVM_OP_COUNT_;
   }
@@ -619,9 +645,12 @@ ppvm_status validate(const ppvm_sum* s, const ppvm_op& op) {
   if (op.code >= PPVM_OP_COUNT_) return fail(PPVM_EINVAL, "unknown op code");
   if (op.code == PPVM_OP_TRUNCATE) return PPVM_OK;
   if (op.q0 >= s->n) return fail(PPVM_EINVAL, "qubit index out of range");
+  const bool loss_op = op.code == PPVM_OP_LOSS_CHANNEL || op.code == PPVM_OP_RESET_LOSS_CHANNEL ||
+                       op.code == PPVM_OP_CORRELATED_LOSS_CHANNEL;
+  if (loss_op && !s->lossy) return fail(PPVM_EINVAL, "loss channels need a lossy sum (PPVM_FLAG_LOSSY)");
   const bool two = op.code == PPVM_OP_CNOT || op.code == PPVM_OP_CZ || op.code == PPVM_OP_CY ||
                    op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY || op.code == PPVM_OP_RZZ ||
-                   op.code == PPVM_OP_DEPOLARIZE2;
+                   op.code == PPVM_OP_DEPOLARIZE2 || op.code == PPVM_OP_CORRELATED_LOSS_CHANNEL;
   if (two && (op.q1 >= s->n || op.q1 == op.q0))
     return fail(PPVM_EINVAL, "two-qubit op needs two distinct qubits in range");
   return PPVM_OK;
@@ -690,7 +719,7 @@ void gen_from_op(const ppvm_sum* s, const ppvm_op& op, Gen& g) {
     case PPVM_OP_RZZ: set(op.q0, false, true); set(op.q1, false, true); break;
     default: break;
   }
-  (void)s;
+  g.lw = s->lossy ? (uint32_t)s->wr : 0u;
 }
 
 // ---- Clifford tableau of a run (host) ------------------------------------------------------------
@@ -849,6 +878,46 @@ struct K {
     s->n_ub = std::min<unsigned long long>(s->cap, 2 * s->n_ub);
   }
 
+  // LossChannel / ResetLossChannel / CorrelatedLossChannel (noise.rs:165-275) on a lossy sum:
+  // see loss.cuh.  Writes the whole output into the alternate planes, then swaps.
+  static void loss(ppvm_sum* s, const ppvm_op& o, int op) {
+    const Planes P = s->planes_view(), O = s->alt_view();
+    const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
+    unsigned long long tsize = next_pow2(std::max<unsigned long long>(2 * nub, 1024));
+    if (tsize > s->table_cap) tsize = s->table_cap;
+    LossOp lo;
+    std::memset(&lo, 0, sizeof(lo));
+    lo.mode = o.code == PPVM_OP_LOSS_CHANNEL ? kLossChannel
+              : o.code == PPVM_OP_RESET_LOSS_CHANNEL ? kResetLoss : kCorrelatedLoss;
+    lo.qa = o.q0;
+    lo.qb = lo.mode == kCorrelatedLoss ? o.q1 : o.q0;
+    lo.lw = (uint32_t)s->wr;
+    if (lo.mode == kLossChannel) {
+      lo.p0 = o.theta;
+      lo.keep1 = 1.0 - o.theta;  // T::Coeff::from(1.0) - p
+    } else if (lo.mode == kCorrelatedLoss) {
+      lo.p0 = o.p[0];
+      lo.p1 = o.p[1];
+      lo.p2 = o.p[2];
+      lo.keep1 = 1.0 - o.p[2];
+      lo.keep0 = 1.0 - o.p[1] * 2.0 - o.p[0];
+    }
+    const unsigned tep = s->next_table_epoch();
+    {
+      ProfScope ps(s, F_LOSS, op, 1);
+      launch(k_loss_index<W>, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, s->table, tsize - 1, tep,
+             op, s->d_log);
+      launch(k_loss_count<W>, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, lo, s->table, tsize - 1,
+             tep);
+      const unsigned e1 = s->next_tile_epoch(), e2 = s->next_tile_epoch();
+      launch(k_loss_emit<W, 256>, grid_for(nub, 256, 8), 256, 0, s->stream, P, O, s->d_ctrl, lo, s->table,
+             tsize - 1, tep, s->tstate, s->tstate2, e1, e2, op, s->d_log);
+    }
+    std::swap(s->planes, s->alt);
+    s->swaps.push_back(op);
+    s->n_ub = std::min<unsigned long long>(s->cap, s->n_ub * (lo.mode == kCorrelatedLoss ? 4 : 2));
+  }
+
   static void clifford(ppvm_sum* s, const DevOp* ops_dev, int nops, int op0) {
     const Planes P = s->planes_view();
     ProfScope ps(s, F_CLIFF, op0, nops);
@@ -863,7 +932,7 @@ struct K {
       launch(k_truncate<W, kScanBlock, ITEMS>, grid_for(std::max<unsigned long long>(s->n_ub, 1), TILE, 8),
              kScanBlock, 0, s->stream,
           P, s->d_ctrl, s->thr, s->maxw, s->d_pres_keys, s->d_pres_table, s->pres_mask, s->npres,
-          s->side, s->tstate, s->next_tile_epoch(), op, s->d_log);
+          s->side, s->tstate, s->next_tile_epoch(), op, s->d_log, s->maxlw, s->lossy ? (unsigned)s->wr : 0u);
     }
     ProfScope ps2(s, F_COMMIT, op, 1);
     launch(k_commit_truncate<W>, 1, 256, 0, s->stream, P, s->d_ctrl, s->side, op, s->d_log);
@@ -1009,7 +1078,7 @@ struct K {
   }
   static void trace(ppvm_sum* s, int nblocks, int nitems) {
     k_trace<W><<<nblocks, kRedBlock, 0, s->stream>>>(s->planes_view(), s->d_ctrl, s->d_pat, nitems,
-                                                     s->n, s->d_partials);
+                                                     s->n, s->d_partials, s->lossy ? (unsigned)s->wr : 0u);
     k_sum_partials<<<1, kRedBlock, 0, s->stream>>>(s->d_partials, nblocks, s->d_ctrl);
   }
   static void weights(ppvm_sum* s, uint32_t* out) {
@@ -1094,6 +1163,15 @@ ppvm_status clear_err(ppvm_sum* s) {
   return PPVM_OK;
 }
 
+// Whether a local op can join a composed Clifford (tableau) pass: a Clifford map applied to
+// every term alike.  On a lossy sum a two-qubit gate leaves terms with a lost qubit alone, so
+// its map depends on the term: those ops take the per-op pass.
+bool tab_ok(const ppvm_sum* s, const DevOp& d) {
+  if (!is_cliff_code(d.code)) return false;
+  if (!s->lossy) return true;
+  return !(d.code == C_CNOT || d.code == C_CZ || d.code == C_CY || (d.code == C_ROTC && d.two));
+}
+
 // Enqueues ops[start..n) (gate-list indices start..n).  Generators of explicit Pauli rotations
 // come from `gens` when ops[i].flags == 1 (index in q0).
 ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
@@ -1129,10 +1207,11 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
     size_t a = 0, pend = 0;  // run[pend, a) waits for the per-op pass
     while (a < run.size()) {
       size_t b = a;
-      while (b < run.size() && is_cliff_code(run[b].code)) ++b;
+      while (b < run.size() && tab_ok(s, run[b])) ++b;
       if (b - a >= (size_t)kTabMinOps) {
         PPVM_TRY(per_op(pend, a));
-        const int t_op = (b == run.size() && trunc_op >= 0 && s->npres == 0) ? trunc_op : -1;
+        const int t_op =
+            (b == run.size() && trunc_op >= 0 && s->npres == 0 && s->maxlw == UINT64_MAX) ? trunc_op : -1;
         HostTableau tab;
         compose_tableau(s->W, run.data() + a, (int)(b - a), tab);
         PPVM_TRY(enqueue_tableau(s, tab, run_start + (int)a, (int)(b - a), t_op));
@@ -1171,12 +1250,22 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
       DISPATCH_W(s->W, damping(s, op.q0, op.theta, (int)i));
       continue;
     }
-    if (is_local(s, op)) {
-      if (run.empty()) run_start = (int)i;
-      run.push_back(to_devop(op));
+    if (op.code == PPVM_OP_LOSS_CHANNEL || op.code == PPVM_OP_RESET_LOSS_CHANNEL ||
+        op.code == PPVM_OP_CORRELATED_LOSS_CHANNEL) {
+      PPVM_TRY(flush(-1, nullptr));
+      DISPATCH_W(s->W, loss(s, op, (int)i));
       continue;
     }
-    // fused run of single-qubit RX (or RZ) rotations on distinct qubits
+    if (is_local(s, op)) {
+      if (run.empty()) run_start = (int)i;
+      DevOp d = to_devop(op);
+      d.lw = s->lossy ? (uint16_t)s->wr : (uint16_t)0;
+      run.push_back(d);
+      continue;
+    }
+    // fused run of single-qubit RX (or RZ) rotations on distinct qubits.  Not on a lossy sum:
+    // its correlated loss channel sums up to three children per key in the reference's term
+    // order, which a fused run (same terms, another order) would change in the last bit.
     const auto cap_it = s->run_cap.find(i);
     int max_gates = cap_it == s->run_cap.end() ? kRunMaxGates : cap_it->second;
     if (max_gates < 0) {  // the run starting here goes gate by gate: -max_gates gates
@@ -1184,7 +1273,7 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
       max_gates = 0;
     }
     const bool fusable = (op.code == PPVM_OP_RX || op.code == PPVM_OP_RZ) &&
-                         !(s->flags & PPVM_FLAG_EXACT_ORDER) && s->npres == 0 && max_gates >= 2 &&
+                         !(s->flags & PPVM_FLAG_EXACT_ORDER) && !s->lossy && s->npres == 0 && max_gates >= 2 &&
                          i >= per_gate_end;
     if (fusable) {
       RunDesc rd;
@@ -1203,7 +1292,9 @@ ppvm_status enqueue(ppvm_sum* s, const ppvm_op* ops, size_t n_ops, size_t start,
       }
       if (rd.L >= 2) {
         PPVM_TRY(flush(-1, nullptr));
-        const int trunc_op = (j < n_ops && ops[j].code == PPVM_OP_TRUNCATE && ops[j].flags == 0) ? (int)j : -1;
+        const int trunc_op =
+            (j < n_ops && ops[j].code == PPVM_OP_TRUNCATE && ops[j].flags == 0 && s->maxlw == UINT64_MAX) ? (int)j
+                                                                                                      : -1;
         PPVM_TRY(enqueue_run(s, rd, (int)i, (int)rd.L, trunc_op));
         s->run_len[i] = (int)rd.L;
         i = trunc_op >= 0 ? j : j - 1;  // the loop's ++i moves past the run (and its TRUNCATE)
@@ -1414,12 +1505,18 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
   *out = nullptr;
   if (n_qubits == 0 || n_qubits > 64 * kMaxW)
     return fail(PPVM_EINVAL, "n_qubits must be in [1, 512]");
+  const bool lossy = (flags & PPVM_FLAG_LOSSY) != 0;
+  if (lossy && n_qubits > 32 * kMaxW) return fail(PPVM_EINVAL, "a lossy sum holds at most 256 qubits");
   PPVM_TRY(ensure_device(device));
-  const int W = (int)((n_qubits + 63) / 64);
+  const int wr = (int)((n_qubits + 63) / 64);
+  const int W = lossy ? 2 * wr : wr;  // a lossy sum keeps its loss bits in the X plane's upper words
   if (ppvm_sum* c = take_cached(device, W)) {  // a cached handle: reset its state
     c->n = n_qubits;
+    c->wr = wr;
+    c->lossy = lossy;
     c->thr = min_abs_coeff;
     c->maxw = max_weight;
+    c->maxlw = UINT64_MAX;
     c->flags = flags;
     c->n_host = c->n_ub = 0;
     c->poisoned = false;
@@ -1447,6 +1544,8 @@ ppvm_status ppvm_sum_create2(ppvm_sum** out, uint32_t n_qubits, double min_abs_c
   s->device = device;
   s->n = n_qubits;
   s->W = W;
+  s->wr = wr;
+  s->lossy = lossy;
   s->thr = min_abs_coeff;
   s->maxw = max_weight;
   s->flags = flags;
@@ -1599,6 +1698,7 @@ ppvm_status ppvm_sum_clone(const ppvm_sum* src, ppvm_sum** out) {
                              sizeof(uint64_t) * src->n_host, cudaMemcpyDeviceToDevice, d->stream));
   d->n_host = src->n_host;
   d->n_ub = src->n_host;
+  d->maxlw = src->maxlw;
   PPVM_TRY(init_ctrl(d, src->n_host));
   if (src->npres) {
     std::vector<uint64_t> x, z;
@@ -1626,12 +1726,7 @@ ppvm_status ppvm_sum_add_terms(ppvm_sum* s, const uint64_t* x, const uint64_t* z
   if (!x || !z || !c) return fail(PPVM_EINVAL, "null term arrays");
   if (s->poisoned) return fail(PPVM_ECUDA, "sum is in an error state from an earlier failure");
   const int W = s->W;
-  // bits beyond n must be clear
-  const int tail = (int)(s->n % 64);
-  for (size_t i = 0; i < k; ++i) {
-    if (tail && ((x[i * W + W - 1] | z[i * W + W - 1]) >> tail))
-      return fail(PPVM_EINVAL, "word has bits set at or above n_qubits");
-  }
+  PPVM_TRY(check_words(s, x, z, k));
   PPVM_TRY(ensure_device(s->device));
   if (s->n_host + k > s->cap) PPVM_TRY(grow(s, std::max<unsigned long long>(2 * s->cap, s->n_host + k + 1024)));
   // the new terms go up through the pinned upload arena (the stream is idle between calls)
@@ -1674,6 +1769,7 @@ ppvm_status ppvm_sum_add_string(ppvm_sum* s, const char* word, double c) {
     if (ch == 'X') x[q >> 6] |= b;
     else if (ch == 'Z') z[q >> 6] |= b;
     else if (ch == 'Y') { x[q >> 6] |= b; z[q >> 6] |= b; }
+    else if (ch == 'L' && s->lossy) x[s->wr + (q >> 6)] |= b;
     else if (ch != 'I') return fail(PPVM_EINVAL, std::string("Invalid Pauli character: ") + ch);
     ++q;
   }
@@ -1838,6 +1934,27 @@ ppvm_status ppvm_depolarize2(ppvm_sum* s, const uint32_t* t, size_t k, double p,
   return run_gate(s, PPVM_OP_DEPOLARIZE2, t, k, true, p, nullptr, truncate);
 }
 
+// Loss channels of lossy sums (noise.rs:165-275), one call per target list like the other
+// channels: the reference's Python binding applies each to one qubit (or pair) and truncates.
+ppvm_status ppvm_loss_channel(ppvm_sum* s, const uint32_t* t, size_t k, double p, int truncate) {
+  return run_gate(s, PPVM_OP_LOSS_CHANNEL, t, k, false, p, nullptr, truncate);
+}
+ppvm_status ppvm_reset_loss_channel(ppvm_sum* s, const uint32_t* t, size_t k, int truncate) {
+  return run_gate(s, PPVM_OP_RESET_LOSS_CHANNEL, t, k, false, 0.0, nullptr, truncate);
+}
+ppvm_status ppvm_correlated_loss_channel(ppvm_sum* s, const uint32_t* t, size_t k, const double p[3],
+                                         int truncate) {
+  if (!p) return fail(PPVM_EINVAL, "null probabilities");
+  return run_gate(s, PPVM_OP_CORRELATED_LOSS_CHANNEL, t, k, true, 0.0, p, truncate);
+}
+ppvm_status ppvm_sum_set_max_loss_weight(ppvm_sum* s, uint64_t max_loss_weight) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  if (!s->lossy && max_loss_weight != UINT64_MAX)
+    return fail(PPVM_EINVAL, "a loss-weight cap needs a lossy sum (PPVM_FLAG_LOSSY)");
+  s->maxlw = max_loss_weight;
+  return PPVM_OK;
+}
+
 // The factor of each (P_a, P_b), code x | z << 1 per qubit, is 1 - 2 p[i1] - ... - 2 p[i8] over
 // the eight two-qubit Paulis that anticommute with it, subtracted in the order the reference
 // writes them (noise.rs:50-99; the order fixes the rounding).  p indices name IX IY IZ XI XX
@@ -1905,9 +2022,11 @@ ppvm_status ppvm_amplitude_damping(ppvm_sum* s, uint32_t q, double gamma, int tr
 
 ppvm_status ppvm_pauli_rotation(ppvm_sum* s, const uint64_t* gx, const uint64_t* gz, double theta, int truncate) {
   if (!s || !gx || !gz) return fail(PPVM_EINVAL, "null argument");
-  const int W = s->W;
+  const int W = s->W, wr = s->wr;
   const int tail = (int)(s->n % 64);
-  if (tail && ((gx[W - 1] | gz[W - 1]) >> tail)) return fail(PPVM_EINVAL, "generator has bits at or above n_qubits");
+  if (tail && ((gx[wr - 1] | gz[wr - 1]) >> tail)) return fail(PPVM_EINVAL, "generator has bits at or above n_qubits");
+  for (int w = wr; w < W; ++w)
+    if (gx[w] | gz[w]) return fail(PPVM_EINVAL, "a generator has no loss bits (the upper words must be 0)");
   bool any = false;
   for (int w = 0; w < W; ++w) any |= (gx[w] | gz[w]) != 0;
   std::vector<Gen> gens(1);
@@ -1916,6 +2035,7 @@ ppvm_status ppvm_pauli_rotation(ppvm_sum* s, const uint64_t* gx, const uint64_t*
     gens[0].gx[w] = gx[w];
     gens[0].gz[w] = gz[w];
   }
+  gens[0].lw = s->lossy ? (uint32_t)wr : 0u;
   std::vector<ppvm_op> ops;
   if (any) {
     if (is_clifford_angle(s, theta)) {

@@ -49,6 +49,25 @@ __device__ __forceinline__ void load_rec(const uint64_t* rec, unsigned long long
   c = __longlong_as_double((long long)r[2 * W]);
 }
 
+// The generator as it acts on the term with X words x: on a lossy sum (g.lw != 0) it skips
+// the term's lost qubits, which is the reference's loss fallback of rotate_2
+// (crates/ppvm-pauli-sum/src/sum/rot2.rs:26-33) extended to any support: a lost qubit has
+// x = z = 0, so the anticommutation test and the sign are those of the full generator and only
+// the child's bits differ.
+template <int W>
+__device__ __forceinline__ void gen_on(const Gen& g, const uint64_t (&x)[W], uint64_t (&gx)[W],
+                                       uint64_t (&gz)[W]) {
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    uint64_t lost = 0;
+#pragma unroll
+    for (int v = 0; v < W; ++v)
+      if (g.lw && v == w + (int)g.lw) lost = x[v];
+    gx[w] = g.gx[w] & ~lost;
+    gz[w] = g.gz[w] & ~lost;
+  }
+}
+
 template <int W>
 struct ItemsFor {
   // terms per thread of a look-back tile: small enough that a sum of 10^5..10^6 terms
@@ -153,13 +172,14 @@ k_rot_pair(Ctrl* ctrl, Gen g, const uint64_t* s_rec, uint32_t* partner,
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
        s += stride) {
-    uint64_t x[W], z[W], px[W], pz[W];
+    uint64_t x[W], z[W], px[W], pz[W], ex[W], ez[W];
     double c;
     load_rec<W>(s_rec, s, x, z, c);
+    gen_on<W>(g, x, ex, ez);
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-      px[w] = x[w] ^ g.gx[w];
-      pz[w] = z[w] ^ g.gz[w];
+      px[w] = x[w] ^ ex[w];
+      pz[w] = z[w] ^ ez[w];
     }
     const bool use_p = key_less<W>(px, pz, x, z);
     uint64_t rx[W], rz[W];
@@ -275,10 +295,12 @@ k_rot_apply(Planes P, Ctrl* ctrl, Gen g, double sn, double cs, const uint32_t* s
         double c;
         load_rec<W>(s_rec, s, x, z, c);
         const double eps = rot_sign<W>(g, x, z);
+        uint64_t ex[W], ez[W];
+        gen_on<W>(g, x, ex, ez);
 #pragma unroll
         for (int w = 0; w < W; ++w) {
-          x[w] ^= g.gx[w];
-          z[w] ^= g.gz[w];
+          x[w] ^= ex[w];
+          z[w] ^= ez[w];
         }
         store_key<W>(P, r, x, z);
         P.c[r] = __dmul_rn(c, eps * sn);
@@ -326,7 +348,7 @@ template <int W, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_truncate(Planes P, Ctrl* ctrl, double thr, unsigned long long maxw, const uint64_t* pres_keys,
            const int* pres_table, unsigned pres_mask, int npres, uint64_t* side,
-           unsigned long long* ts, unsigned epoch, int op, OpLog* log) {
+           unsigned long long* ts, unsigned epoch, int op, OpLog* log, unsigned long long maxlw, unsigned lw) {
   pdl_wait();
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
@@ -362,6 +384,13 @@ k_truncate(Planes P, Ctrl* ctrl, double thr, unsigned long long maxw, const uint
         kc[k] = P.c[i];
         keep = !(fabs(kc[k]) < thr);
         if (wcap) keep = keep && (weight<W>(kx[k], kz[k]) <= maxw);
+        if (lw && maxlw != ~0ull) {  // MaxLossWeight: lost qubits, the X plane's upper words
+          unsigned lost = 0;
+#pragma unroll
+          for (int w = 0; w < W; ++w)
+            if (w >= (int)lw) lost += __popcll(kx[k][w]);
+          keep = keep && lost <= maxlw;
+        }
         if (!keep && npres > 0) sd = preserved<W>(kx[k], kz[k], pres_keys, pres_table, pres_mask);
       }
       keep_b[k] = __ballot_sync(kFull, keep);
@@ -436,7 +465,8 @@ struct DevOp {
   uint32_t code;
   uint16_t w0, b0, w1, b1;
   uint16_t ax, az;  // bit0: qubit0, bit1: qubit1 (axis of C_ROTC)
-  uint16_t two, pad;
+  uint16_t two;
+  uint16_t lw;      // lossy sums: first loss word of the X plane (two-qubit ops skip lost qubits)
   double f0, f1, f2;
 };
 
@@ -478,6 +508,18 @@ k_clifford(Planes P, Ctrl* ctrl, const DevOp* ops, int nops, int op0, OpLog* log
       const uint64_t m0 = 1ull << d.b0, m1 = 1ull << d.b1;
       uint64_t x0w = s_x[d.w0][t], z0w = s_z[d.w0][t];
       const bool x0 = x0w & m0, z0 = z0w & m0;
+      // lossy sums: which of the op's qubits are lost.  One-qubit ops need no test (a lost
+      // qubit has x = z = 0, which every one-qubit rule leaves alone); two-qubit Cliffords,
+      // depolarize2 and the two-qubit Pauli error skip the term (phase/clifford.rs:77,92,168;
+      // noise.rs:98-102,122); a Clifford-angle rotation acts on the qubits that are not lost.
+      bool l0 = false, l1 = false;
+      if (d.lw) {
+        const bool skip2 = d.code == C_CNOT || d.code == C_CZ || d.code == C_CY || d.code == C_DEP2 ||
+                           d.code == C_PERR2;
+        l0 = s_x[d.lw + d.w0][t] & m0;
+        l1 = (skip2 || (d.code == C_ROTC && d.two)) ? (bool)(s_x[d.lw + d.w1][t] & m1) : false;
+        if ((l0 || l1) && skip2) continue;
+      }
       switch (d.code) {
         case C_X: neg ^= z0; break;
         case C_Y: neg ^= x0 ^ z0; break;
@@ -544,13 +586,13 @@ k_clifford(Planes P, Ctrl* ctrl, const DevOp* ops, int nops, int op0, OpLog* log
           break;
         }
         case C_ROTC: {
-          const bool ax0 = d.ax & 1, az0 = d.az & 1;
+          const bool ax0 = (d.ax & 1) && !l0, az0 = (d.az & 1) && !l0;
           bool x1 = false, z1 = false, ax1 = false, az1 = false;
           if (d.two) {
             x1 = s_x[d.w1][t] & m1;
             z1 = s_z[d.w1][t] & m1;
-            ax1 = (d.ax >> 1) & 1;
-            az1 = (d.az >> 1) & 1;
+            ax1 = ((d.ax >> 1) & 1) && !l1;
+            az1 = ((d.az >> 1) & 1) && !l1;
           }
           const bool anti = ((x0 & az0) ^ (z0 & ax0)) ^ ((x1 & az1) ^ (z1 & ax1));
           if (!anti) break;
@@ -648,9 +690,25 @@ __device__ __forceinline__ unsigned pauli_code(const uint64_t (&x)[W], const uin
   return (unsigned)((xw >> (q & 63)) & 1u) | ((unsigned)((zw >> (q & 63)) & 1u) << 1);
 }
 
+// Pattern code of qubit q: pauli_code, or 4 for a lost qubit of a lossy sum (lw: first loss
+// word of the X plane, 0 for a plain sum).  No pattern item accepts 4 (accept masks have four
+// bits): L matches no Pauli pattern (crates/ppvm-pauli-word/src/pattern/contains.rs:25-41).
+template <int W>
+__device__ __forceinline__ unsigned pat_code(const uint64_t (&x)[W], const uint64_t (&z)[W], unsigned lw,
+                                             unsigned q) {
+  if (lw) {
+    uint64_t l = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+      if ((int)(lw + (q >> 6)) == w) l = x[w];
+    if ((l >> (q & 63)) & 1u) return 4u;
+  }
+  return pauli_code<W>(x, z, q);
+}
+
 template <int W>
 __device__ bool pattern_match(const PatItem* items, int nitems, unsigned n, const uint64_t (&x)[W],
-                              const uint64_t (&z)[W]) {
+                              const uint64_t (&z)[W], unsigned lw) {
   unsigned pos = 0;
   for (int it = 0; it < nitems; ++it) {
     const PatItem p = items[it];
@@ -658,7 +716,7 @@ __device__ bool pattern_match(const PatItem* items, int nitems, unsigned n, cons
       bool next = false;
       while (pos < n) {
         const unsigned q = pos++;
-        const unsigned c = pauli_code<W>(x, z, q);
+        const unsigned c = pat_code<W>(x, z, lw, q);
         if (q == p.arg) {
           next = (p.accept >> c) & 1u;
           break;
@@ -668,12 +726,12 @@ __device__ bool pattern_match(const PatItem* items, int nitems, unsigned n, cons
       }
       if (!next) return false;
     } else if (p.kind == 1) {
-      while (pos < n && ((p.accept >> pauli_code<W>(x, z, pos)) & 1u)) ++pos;
+      while (pos < n && ((p.accept >> pat_code<W>(x, z, lw, pos)) & 1u)) ++pos;
     } else {
       unsigned long long matched = 0;
       bool done = false;
       while (pos < n) {
-        if ((p.accept >> pauli_code<W>(x, z, pos)) & 1u) {
+        if ((p.accept >> pat_code<W>(x, z, lw, pos)) & 1u) {
           ++pos;
           if (++matched == p.arg) {
             done = true;
@@ -689,13 +747,14 @@ __device__ bool pattern_match(const PatItem* items, int nitems, unsigned n, cons
     }
   }
   for (; pos < n; ++pos)
-    if (pauli_code<W>(x, z, pos) != 0) return false;
+    if (pat_code<W>(x, z, lw, pos) != 0) return false;
   return true;
 }
 
 template <int W>
 __global__ void __launch_bounds__(256)
-k_trace(Planes P, const Ctrl* ctrl, const PatItem* items, int nitems, unsigned nq, double* partials) {
+k_trace(Planes P, const Ctrl* ctrl, const PatItem* items, int nitems, unsigned nq, double* partials,
+        unsigned lw) {
   __shared__ double s_red[8];
   const unsigned long long N = ld_volatile(&ctrl->n);
   double acc = 0.0;
@@ -703,7 +762,7 @@ k_trace(Planes P, const Ctrl* ctrl, const PatItem* items, int nitems, unsigned n
        i += (unsigned long long)gridDim.x * blockDim.x) {
     uint64_t x[W], z[W];
     load_key<W>(P, i, x, z);
-    if (pattern_match<W>(items, nitems, nq, x, z)) acc = __dadd_rn(acc, P.c[i]);
+    if (pattern_match<W>(items, nitems, nq, x, z, lw)) acc = __dadd_rn(acc, P.c[i]);
   }
   const double b = block_sum(acc, s_red);
   if (threadIdx.x == 0) partials[blockIdx.x] = b;

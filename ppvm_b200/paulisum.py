@@ -23,7 +23,7 @@ from typing import Any
 import numpy as np
 
 from . import gates as G
-from ._lib import EINVAL, FLAG_CLIFFORD_ANGLES, FLAG_EXACT_ORDER, OK, UMAX, Op, PPVMError, lib
+from ._lib import EINVAL, FLAG_CLIFFORD_ANGLES, FLAG_EXACT_ORDER, FLAG_LOSSY, OK, UMAX, Op, PPVMError, lib
 
 _COMPACT_RE = re.compile(r"^([IXYZ]\d+)+$")
 _COMPACT_TOKEN_RE = re.compile(r"([IXYZ])(\d+)")
@@ -99,8 +99,6 @@ class PauliSum:
                  max_loss_weight: int | None = None, preserve_strings: Sequence[str] | None = None,
                  *, clifford_angles: bool = False, exact_order: bool = False, device: int = 0,
                  capacity: int = 0):
-        if max_loss_weight is not None:
-            raise NotImplementedError("lossy Pauli words are not supported by this engine")
         if not initial_terms:
             raise ValueError("At least one term must be provided to initialize PauliSum.")
         for term in initial_terms:
@@ -116,14 +114,19 @@ class PauliSum:
         self.coefficients = tuple(float(c) for c in coefficients)
         self.min_abs_coeff = float(min_abs_coeff)
         self.max_pauli_weight = max_pauli_weight
-        self.max_loss_weight = None
+        # the plain tiers accept max_loss_weight and ignore it, as the reference's binding does
+        # (crates/ppvm-python-native/src/interface.rs:89); LossyPauliSum applies it
+        self.max_loss_weight = max_loss_weight
         self.preserve_strings = list(preserve_strings) if preserve_strings else None
-        self.W = G.words(self.n_qubits)
+        self.W = G.lossy_words(self.n_qubits) if self._LOSSY else G.words(self.n_qubits)
         self._h = ctypes.c_void_p()
         mw = UMAX if max_pauli_weight is None else int(max_pauli_weight)
         flags = (FLAG_CLIFFORD_ANGLES if clifford_angles else 0) | (FLAG_EXACT_ORDER if exact_order else 0)
+        flags |= FLAG_LOSSY if self._LOSSY else 0
         self._check(lib().ppvm_sum_create2(ctypes.byref(self._h), self.n_qubits, self.min_abs_coeff, mw,
                                            int(capacity), flags, int(device)))
+        if self._LOSSY and max_loss_weight is not None:
+            self._check(lib().ppvm_sum_set_max_loss_weight(self._h, int(max_loss_weight)))
         if self.preserve_strings:
             for s in self.preserve_strings:
                 if len(s) != n_qubits:
@@ -155,11 +158,19 @@ class PauliSum:
             raise ValueError(msg)
         raise PPVMError(status, msg)
 
+    _LOSSY = False  # LossyPauliSum: words over I, X, Y, Z and L
+
+    def _parse(self, w):
+        return G.parse_lossy_word(w, self.n_qubits) if self._LOSSY else G.parse_word(w, self.n_qubits)
+
+    def _word(self, x, z) -> str:
+        return G.lossy_word_str(x, z, self.n_qubits) if self._LOSSY else G.word_str(x, z, self.n_qubits)
+
     def _planes(self, words):
         x = np.zeros((len(words), self.W), dtype=np.uint64)
         z = np.zeros((len(words), self.W), dtype=np.uint64)
         for i, w in enumerate(words):
-            x[i], z[i] = G.parse_word(w, self.n_qubits)
+            x[i], z[i] = self._parse(w)
         return x, z
 
     def __del__(self):
@@ -214,7 +225,7 @@ class PauliSum:
     @property
     def terms(self) -> list[tuple[str, float]]:
         x, z, c = self.export()
-        return [(G.word_str(x[i], z[i], self.n_qubits), float(c[i])) for i in range(len(c))]
+        return [(self._word(x[i], z[i]), float(c[i])) for i in range(len(c))]
 
     def weights(self) -> list[tuple[str, int]]:
         x, z, _ = self.export()
@@ -223,7 +234,7 @@ class PauliSum:
         got = ctypes.c_size_t()
         self._check(lib().ppvm_weights(self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), n,
                                        ctypes.byref(got)))
-        return [(G.word_str(x[i], z[i], self.n_qubits), int(w[i])) for i in range(got.value)]
+        return [(self._word(x[i], z[i]), int(w[i])) for i in range(got.value)]
 
     def current_max_weight(self) -> int:
         out = ctypes.c_uint64()
@@ -302,6 +313,9 @@ class PauliSum:
         """exp(-i theta/2 P) for a Pauli string P of length n (or compact, e.g. "X0Z3")."""
         word, _ = _parse_term(pauli, self.n_qubits)
         gx, gz = G.parse_word(word, self.n_qubits)
+        if self._LOSSY:  # the generator has no loss bits: the upper words stay 0
+            gx = np.concatenate([gx, np.zeros_like(gx)])
+            gz = np.concatenate([gz, np.zeros_like(gz)])
         self._check(lib().ppvm_pauli_rotation(self._h, _p64(gx), _p64(gz), float(theta), int(bool(truncate))))
 
     # ---- noise (diagonal channels) --------------------------------------------------------------
@@ -419,6 +433,35 @@ class PauliSum:
 OP_DTYPE = np.dtype([("code", "<u4"), ("q0", "<u4"), ("q1", "<u4"), ("flags", "<u4"),
                      ("theta", "<f8"), ("p", "<f8", (3,))])
 assert OP_DTYPE.itemsize == ctypes.sizeof(Op)
+
+
+class LossyPauliSum(PauliSum):
+    """A PauliSum of lossy words: each qubit is I, X, Y, Z or L (lost), as the reference's
+    ``ppvm.LossyPauliSum`` (ppvm-python/src/ppvm/paulisum.py:419-499) over LossyPauliWord
+    (crates/ppvm-pauli-word/src/loss/data.rs).  ``max_loss_weight`` caps the number of L per
+    term at truncation.  At most 256 qubits.  The loss channels take the reference's
+    arguments; gates treat L as the reference does (a lost qubit is left alone)."""
+
+    _LOSSY = True
+
+    def loss_channel(self, addr0: int, p: float, *, truncate: bool = True) -> None:
+        """L -> L + p I on ``addr0``; I, X, Y, Z -> (1 - p) (noise.rs:165-181)."""
+        arr, k = _u32([int(addr0)])
+        self._check(lib().ppvm_loss_channel(self._h, arr, k, float(p), int(bool(truncate))))
+
+    def correlated_loss_channel(self, addr0: int, addr1: int, p, *, truncate: bool = True) -> None:
+        """Correlated loss of the pair (noise.rs:184-243); p = (both, one, second after first)."""
+        pv = [float(v) for v in p]
+        if len(pv) != 3:
+            raise ValueError("correlated_loss_channel needs 3 probabilities")
+        arr, k = _u32([int(addr0), int(addr1)])
+        self._check(lib().ppvm_correlated_loss_channel(self._h, arr, k, (ctypes.c_double * 3)(*pv),
+                                                       int(bool(truncate))))
+
+    def reset_loss_channel(self, addr0: int, *, truncate: bool = True) -> None:
+        """L -> 0 on ``addr0``; I, Z -> themselves + L (noise.rs:245-275)."""
+        arr, k = _u32([int(addr0)])
+        self._check(lib().ppvm_reset_loss_channel(self._h, arr, k, int(bool(truncate))))
 
 
 class GateList:
