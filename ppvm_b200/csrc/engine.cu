@@ -801,6 +801,20 @@ void compose_tableau(int W, const DevOp* d, int L, HostTableau& t) {
     t.sign[row] = neg ? 1 : 0;
     t.ph[row] = (uint8_t)((p + (neg ? 2u : 0u)) & 3u);
   }
+  // generators whose image is themselves (same word, phase 0) stay out of the kernel's product
+  for (int c = 0; c < nt; ++c) {
+    const uint32_t q = t.tq[c];
+    for (int pl = 0; pl < 2; ++pl) {
+      const int row = 2 * c + pl;
+      const uint64_t* e = &t.rows[(size_t)row * 2 * W];
+      bool self = t.ph[row] == 0;
+      for (int w = 0; w < W && self; ++w) {
+        const uint64_t bit = (w == (int)(q >> 6)) ? 1ull << (q & 63) : 0ull;
+        self = e[w] == (pl == 0 ? bit : 0ull) && e[W + w] == (pl == 1 ? bit : 0ull);
+      }
+      if (!self) (pl == 0 ? t.tp.Tx : t.tp.Tz)[q >> 6] |= 1ull << (q & 63);
+    }
+  }
 }
 
 // ---- kernel enqueue (templated on W) ------------------------------------------------------------
@@ -996,7 +1010,15 @@ struct K {
     const unsigned long long scratch_min = allow ? smin : ~0ull;
     {
       ProfScope ps(s, F_RUN_GROUPS, op0, L);
-      launch(k_run_groups<W>, grid_for(nub, kRunWarps, 8), kRunWarps * 32, 0, s->stream,
+      // no more blocks than fit on the GPU at once: warps take groups by ticket, so blocks
+      // beyond that would only queue on the ticket counter
+      static int resident = 0;  // blocks per SM (the same on every B200)
+      if (!resident) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_run_groups<W>, kRunWarps * 32, 0) !=
+                cudaSuccess || resident < 1)
+          resident = 1;
+      }
+      launch(k_run_groups<W>, grid_for(nub, kRunWarps, std::min(resident, 8)), kRunWarps * 32, 0, s->stream,
           O, S, s->d_ctrl, d_rd, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0,
           trunc_op, s->d_log, scratch_min);  // its last block publishes the counts and the op log
     }

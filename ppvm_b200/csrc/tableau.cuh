@@ -104,33 +104,44 @@ __host__ __device__ inline bool is_cliff_code(uint32_t code) {
 // ---- device side --------------------------------------------------------------------------
 struct TabParams {
   uint64_t T[kMaxW];    // touched qubits (support of the run)
+  uint64_t Tx[kMaxW];   // touched qubits whose X_q image is not X_q itself
+  uint64_t Tz[kMaxW];   // touched qubits whose Z_q image is not Z_q itself
   uint32_t pre[kMaxW];  // touched qubits in words < w (rank prefix)
   uint32_t nrows;       // 2 * touched: row 2r = image of X_q, 2r+1 = image of Z_q (r = rank of q)
 };
 
 // Maps the word (x, z) through the composed run: (ox, oz) receives the image word, and the
 // return value e is the sign's phase, image = i^e * (Hermitian word): e = 0 or 2 (sign -1);
-// an odd e would mean a broken table.  rows/ph: the image table (shared or global memory).
+// an odd e would mean a broken table.  rows/ph: the image table (shared memory).
+//
+// Generators whose image is themselves are left out of the product: bits outside Tx (X) and
+// Tz (Z) stay as they are.  The product takes the X images before the Z images, so a kept
+// Z_q passes the X images; it anticommutes only with the image of X_q (images keep the
+// commutation of their generators), which contributes a sign where x_q = z_q = 1, q in Tx
+// and not in Tz.
 template <int W>
 __device__ __forceinline__ unsigned tab_map(const uint64_t* rows, const uint8_t* ph, const TabParams& tp,
                                             const uint64_t (&x)[W], const uint64_t (&z)[W], uint64_t (&ox)[W],
                                             uint64_t (&oz)[W]) {
   unsigned p = 0;
+  uint64_t m[2 * W];
 #pragma unroll
   for (int w = 0; w < W; ++w) {
-    p += __popcll(x[w] & z[w]);
-    ox[w] = x[w] & ~tp.T[w];
-    oz[w] = z[w] & ~tp.T[w];
+    p += __popcll(x[w] & z[w]) + 2u * __popcll(x[w] & z[w] & tp.Tx[w] & ~tp.Tz[w]);
+    ox[w] = x[w] & ~tp.Tx[w];
+    oz[w] = z[w] & ~tp.Tz[w];
+    m[w] = x[w] & tp.Tx[w];
+    m[W + w] = z[w] & tp.Tz[w];
   }
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-      uint64_t m = (s == 0 ? x[w] : z[w]) & tp.T[w];
-      while (m) {
-        const int b = __ffsll((long long)m) - 1;
-        m &= m - 1;
-        const unsigned row = 2u * (tp.pre[w] + __popcll(tp.T[w] & ((1ull << b) - 1ull))) + s;
+      uint64_t mk = m[s * W + w];
+      while (mk) {
+        const int b = __ffsll((long long)mk) - 1;
+        mk &= mk - 1;
+        const unsigned row = 2u * (tp.pre[w] + __popcll(tp.T[w] & ((1ull << b) - 1ull))) + (unsigned)s;
         const uint64_t* e = rows + (size_t)row * 2 * W;
         unsigned t = 0;
 #pragma unroll
