@@ -311,12 +311,16 @@ def batched_shard_seed(rank: int) -> int:
     return 1 + rank
 
 
-# DRAM bytes (read + write) of one launch of the kernel, from one ncu capture of this workload
-# (profiles/k_run_groups_kicked_ising_12x12.md and k_tableau_kicked_ising_12x12.md: a layer
-# with about 2e5 terms entering).  Far below the algorithmic bytes: the sum stays in L2.
-CAPTURED_TRAFFIC = {"run_groups": 379648 + 14336, "tableau": 3266560 + 256}
-TRAFFIC_SOURCE = ("ncu --set full capture of one launch of each kernel (the first two matches after skipping "
-                  "76, command in profiles/), dram__bytes_read.sum + dram__bytes_write.sum")
+# DRAM bytes (read + write) per launch of the dominant kernel, per workload: the mean over the
+# kernel's launches in one step, from an ncu capture of this code (dram__bytes_read.sum +
+# dram__bytes_write.sum of every launch of the kernel in the step).  Filled from a capture of
+# the current kernels; a workload or kernel without an entry reports null.
+CAPTURED_TRAFFIC: dict = {
+    "kicked_ising_2d": {"run_groups": 66548 + 402, "tableau": 237986 + 0},          # 21 and 19 launches
+    "clifford_t": {"run_groups": 7685530 + 5397443, "tableau": 8022518 + 3209472},  # 25 and 25 launches
+}
+TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none over one step "
+                  "of this workload (every launch of the kernel), mean per launch")
 
 
 def measured_peak():
@@ -455,8 +459,8 @@ def run_gpu(args):
             achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9
             roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
                     "frac": achieved / peak_gbs, "peak_kind": peak_kind,
-                    "traffic": CAPTURED_TRAFFIC.get(dom),
-                    "traffic_source": TRAFFIC_SOURCE if dom in CAPTURED_TRAFFIC else None,
+                    "traffic": CAPTURED_TRAFFIC.get(args.workload, {}).get(dom),
+                    "traffic_source": TRAFFIC_SOURCE if dom in CAPTURED_TRAFFIC.get(args.workload, {}) else None,
                     "bytes_per_launch": d["bytes"] / d["launches"],
                     "avg_launch_us": 1e3 * d["ms"] / d["launches"],
                     "share_of_device_time": d["ms"] / (1e3 * prof_s) if prof_s else None,
