@@ -292,12 +292,13 @@ ppvm_status ppvm_mlp_predict(ppvm_mlp* mlp, const float* feats, size_t n, float*
 /* Many independent PauliSums (instances), each with its own qubit count, truncation
  * strategy, initial terms and gate list, advanced together on one GPU: one CTA per
  * instance, one launch per Trotter layer (a layer ends at every second TRUNCATE of an
- * instance's list), the layer launches captured once as CUDA graphs.  Each instance's
- * result equals a ppvm_sum run of the same list with PPVM_FLAG_EXACT_ORDER: same terms in
- * the same order, same coefficients.  The reference runs such sets one PauliSum at a time
+ * instance's list).  Each instance's result equals a ppvm_sum run of the same list with
+ * PPVM_FLAG_EXACT_ORDER: same terms in the same order, same coefficients.  The reference runs such sets one PauliSum at a time
  * (its benches loop over circuits, `crates/ppvm-pauli-sum/benches/trotter.rs:28-44`); there
- * is no batch object in the reference.  Supported ops: all op codes, without explicit
- * generators; preserve strings are not supported.  Instances have up to 512 qubits. */
+ * is no batch object in the reference.  Supported ops: Cliffords, rotations, Pauli-error and
+ * depolarising channels, TRUNCATE (no amplitude damping or loss channels, no explicit
+ * generators or preserve strings); set_ops refuses the others with PPVM_EINVAL.  Instances
+ * have up to 512 qubits. */
 typedef struct ppvm_batch ppvm_batch; /* opaque */
 ppvm_status ppvm_batch_create(ppvm_batch** out, size_t n_inst, const uint32_t* n_qubits,
                               const double* min_abs_coeff, const uint64_t* max_weight,
@@ -309,7 +310,10 @@ ppvm_status ppvm_batch_add_terms(ppvm_batch* batch, size_t inst, const uint64_t*
                                  const uint64_t* z, const double* c, size_t k);
 /* Gate list of instance `inst` (as ppvm_gate_list_run takes it). */
 ppvm_status ppvm_batch_set_ops(ppvm_batch* batch, size_t inst, const ppvm_op* ops, size_t n_ops);
-/* Runs every instance from its initial terms through its whole list (layer graphs). */
+/* Runs every instance from its initial terms through its whole list.  Inputs changed by
+ * the setters since the last run (8-byte op records, parameter tables, initial terms) go to
+ * the device in one copy from a pinned staging buffer; the first run of a batch launches the
+ * layers directly, later runs of the unchanged batch replay them as CUDA graphs. */
 ppvm_status ppvm_batch_run(ppvm_batch* batch);
 /* The same in one launch: each CTA runs its instance's whole list. */
 ppvm_status ppvm_batch_run_persistent(ppvm_batch* batch);
@@ -337,10 +341,12 @@ ppvm_status ppvm_batch_term_gate_updates(const ppvm_batch* batch, uint64_t* per_
 ppvm_status ppvm_batch_transfer_counters(const ppvm_batch* batch, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
 /* ---- memory -------------------------------------------------------------------------- */
-/* The large buffers of a sum (term planes, scratch) come from a per-device cache: a
- * destroyed or grown sum gives them back to the cache, and later sums reuse them without
- * cudaMalloc/cudaFree (which synchronise the device).  This call returns every cached buffer
- * to the driver.  No counterpart in the reference (Rust's allocator plays this part). */
+/* The large buffers of a sum (term planes, scratch) and of a batch (term pool, input block)
+ * come from a per-device cache: a destroyed or grown sum or batch gives them back to the
+ * cache, and later ones reuse them without cudaMalloc/cudaFree (which synchronise the
+ * device).  This call returns every cached buffer to the driver, and frees the pinned host
+ * buffer that stages the batches' uploads.  No counterpart in the reference (Rust's
+ * allocator plays this part). */
 ppvm_status ppvm_release_cached_memory(void);
 
 /* ---- diagnostics ------------------------------------------------------------------- */

@@ -5,8 +5,14 @@
 // instance table gives each one its region (offset table).  k_batch runs one Trotter layer
 // of every instance per launch (a layer ends at every second TRUNCATE of the instance's
 // list): CTA b interprets instance b's ops in order, entirely inside the CTA, so the only
-// synchronisation is __syncthreads.  The layer launches are captured once as CUDA graphs
-// and replayed.
+// synchronisation is __syncthreads.  A batch that runs again unchanged replays its layer
+// launches as CUDA graphs.
+//
+// Inputs: each op is an 8-byte record (header word + index into its instance's parameter
+// table), so a list of 10^6 gates is 8 MB; the op records, layer ends, parameter tables and
+// initial terms of all instances travel in one copy from a pinned staging buffer into one
+// device block, and the pool and that block come from the library's buffer cache.  A batch
+// built from host circuits therefore costs little more than its kernels.
 //
 // Per op, with reference semantics (crates/ppvm-pauli-sum/src/sum/data.rs:204-311):
 //   rotation   scan (anticommuting terms, in order) -> pair (partner K^G through an
@@ -24,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -32,6 +39,10 @@
 
 namespace ppvm {
 void set_last_error(const std::string& msg);
+// The per-device buffer cache of the sums (engine.cu): buffers handed back once their
+// stream is idle are reused by later batches and sums without cudaMalloc/cudaFree.
+cudaError_t cache_malloc(void** out, size_t bytes);
+void cache_free(void* p);
 }
 
 using namespace ppvm;
@@ -40,12 +51,47 @@ namespace {
 
 enum BKind : uint32_t { B_ROT = 0, B_LOCAL = 1, B_TRUNC = 2 };
 
-struct BOp {
-  uint32_t kind;
-  uint32_t pad;
-  double sn, cs;  // rotation: sin, cos of theta (host libm, as the reference's f64::sin_cos)
-  DevOp d;        // qubits; rotation axes in ax/az/two; local ops as the per-op pass encodes them
+// One op of an instance's list in 8 bytes: a header word and the index of its first value in
+// the instance's parameter table.  Header: kind:2 | code:5 | two:1 | ax:2 | az:2 | q0:10 |
+// q1:10 (one-qubit ops repeat q0 in q1).  Parameters: rotation sin, cos of theta (host libm,
+// as the reference's f64::sin_cos); Pauli error its three factors; depolarising channels
+// their factor; Clifford-angle rotation the sign of sin.  Consecutive ops with the same
+// values share one entry, so a Trotter list stores a few values per layer.
+struct alignas(8) BOp {
+  uint32_t h;
+  uint32_t param;
 };
+
+constexpr uint32_t bop_header(uint32_t kind, uint32_t code, bool two, uint32_t ax, uint32_t az, uint32_t q0,
+                              uint32_t q1) {
+  return kind | code << 2 | (uint32_t)two << 7 | ax << 8 | az << 10 | q0 << 12 | q1 << 22;
+}
+__device__ __forceinline__ uint32_t bop_kind(uint32_t h) { return h & 3u; }
+
+// The op as the per-op kernels' DevOp (loss word 0: batch instances hold plain words).
+__device__ __forceinline__ DevOp bop_decode(const BOp o, const double* __restrict__ P) {
+  DevOp d;
+  const uint32_t h = o.h;
+  d.code = (h >> 2) & 31u;
+  d.two = (uint16_t)((h >> 7) & 1u);
+  d.ax = (uint16_t)((h >> 8) & 3u);
+  d.az = (uint16_t)((h >> 10) & 3u);
+  const uint32_t q0 = (h >> 12) & 1023u, q1 = h >> 22;
+  d.w0 = (uint16_t)(q0 >> 6);
+  d.b0 = (uint16_t)(q0 & 63u);
+  d.w1 = (uint16_t)(q1 >> 6);
+  d.b1 = (uint16_t)(q1 & 63u);
+  d.lw = 0;
+  d.f0 = d.f1 = d.f2 = 0.0;
+  if (bop_kind(h) == B_LOCAL && d.code >= C_PAULI_ERROR) {
+    d.f0 = P[o.param];
+    if (d.code == C_PAULI_ERROR) {
+      d.f1 = P[o.param + 1];
+      d.f2 = P[o.param + 2];
+    }
+  }
+  return d;
+}
 
 struct BInst {
   unsigned long long off;    // region offset in the pool (u64 words)
@@ -56,6 +102,8 @@ struct BInst {
   unsigned long long need;   // terms needed at a failing op
   double thr;
   unsigned long long maxw;
+  unsigned long long param_off;  // first value of the instance's parameter table
+  unsigned long long init_off;   // its initial terms in the input block (u64 words)
   uint32_t op_begin, op_end, pc, layer_off, n_layers, epoch;
   int err;
   int pad;
@@ -234,8 +282,8 @@ __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v
 // One layer (or, with layer < 0, everything left) of every instance; CTA b = instance b.
 template <int W, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
-k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ layer_ends, int layer,
-        uint64_t* pool) {
+k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ layer_ends,
+        const double* __restrict__ params, int layer, uint64_t* pool) {
   constexpr int NW = BLOCK / 32;
   constexpr unsigned long long TILE = (unsigned long long)BLOCK * ITEMS;
   __shared__ unsigned s_base[ITEMS * NW + 1];
@@ -248,6 +296,7 @@ k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ 
   unsigned pc = I.pc;
   if (pc >= end) return;
   const Region<W> R = region_of<W>(pool, I);
+  const double* __restrict__ P = params + I.param_off;
   const double thr = I.thr;
   const unsigned long long maxw = I.maxw;
   const bool wcap = maxw != ~0ull;
@@ -257,7 +306,8 @@ k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ 
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   while (pc < end) {
-    const uint32_t kind = ops[pc].kind;
+    const BOp op = ops[pc];
+    const uint32_t kind = bop_kind(op.h);
     if (kind == B_TRUNC) {
       // stable in-place compaction: a tile's reads finish (inside tile_ranks) before its
       // writes, and every write goes to a position at or below the word it came from
@@ -295,13 +345,13 @@ k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ 
     }
     if (kind == B_LOCAL) {
       unsigned j = pc;
-      while (j < end && ops[j].kind == B_LOCAL) ++j;
+      while (j < end && bop_kind(ops[j].h) == B_LOCAL) ++j;
       for (unsigned long long i = threadIdx.x; i < N; i += BLOCK) {
         uint64_t x[W], z[W];
         rload<W>(R, i, x, z);
         double c = R.c[i];
         bool neg = false;
-        for (unsigned o = pc; o < j; ++o) local_op<W>(ops[o].d, x, z, c, neg);
+        for (unsigned o = pc; o < j; ++o) local_op<W>(bop_decode(ops[o], P), x, z, c, neg);
         rstore<W>(R, i, x, z);
         R.c[i] = neg ? -c : c;
       }
@@ -311,8 +361,8 @@ k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ 
       continue;
     }
     // ---- rotation exp(-i theta/2 G), G on op.d's one or two qubits ----
-    const DevOp d = ops[pc].d;
-    const double sn = ops[pc].sn, cs = ops[pc].cs;
+    const DevOp d = bop_decode(op, P);
+    const double sn = P[op.param], cs = P[op.param + 1];
     if (++epoch >= 0xFFFFu) {  // pair-table epochs wrapped: clear the table once
       for (unsigned long long t = threadIdx.x; t < R.tsize; t += BLOCK) R.table[t] = 0ull;
       __syncthreads();
@@ -491,13 +541,12 @@ __global__ void __launch_bounds__(256) k_batch_owz(const BInst* insts, uint64_t*
   if (threadIdx.x == 0) out[blockIdx.x] = b;
 }
 
-// Loads initial terms (packed per instance: x[k][W], z[k][W], c[k] at src_off) into regions.
+// Loads initial terms (packed per instance: x[k][W], z[k][W], c[k] at init_off) into regions.
 template <int W>
-__global__ void k_batch_load(const BInst* insts, const unsigned long long* src_off, const uint64_t* src,
-                             uint64_t* pool) {
+__global__ void k_batch_load(const BInst* insts, const uint64_t* src, uint64_t* pool) {
   const BInst& I = insts[blockIdx.x];
   const Region<W> R = region_of<W>(pool, I);
-  const uint64_t* s = src + src_off[blockIdx.x];
+  const uint64_t* s = src + I.init_off;
   const unsigned long long k = I.n;
   for (unsigned long long i = threadIdx.x; i < k; i += blockDim.x) {
 #pragma unroll
@@ -527,6 +576,20 @@ __global__ void k_batch_relocate(const BInst* old_i, const BInst* new_i, uint64_
 
 ppvm_status bfail(ppvm_status s, const std::string& msg) {
   ppvm::set_last_error(msg);
+  return s;
+}
+
+// Page-locked staging for the batches' input uploads: one buffer per process, grown on
+// demand and kept, so that an upload is a memcpy into pinned memory and one DMA copy (no
+// pageable copy through the driver's bounce buffer, no fresh pages to fault in).  An upload
+// holds the lock until its copy has completed.
+struct Staging {
+  std::mutex mu;
+  void* p = nullptr;
+  size_t cap = 0;
+};
+Staging& staging() {
+  static Staging s;
   return s;
 }
 
@@ -566,19 +629,25 @@ struct ppvm_batch {
   std::vector<std::vector<uint64_t>> ix, iz;
   std::vector<std::vector<double>> ic;
   std::vector<std::vector<BOp>> ops;
+  std::vector<std::vector<double>> params;   // parameter table of each instance's ops
   std::vector<std::vector<uint32_t>> lends;  // op index just past each layer's closing TRUNCATE
   std::vector<unsigned long long> cap;       // region capacities (kept across runs)
   // launch configuration (autotuned)
   int block = 256, items = 4, tfac = 2;
-  // device state
+  // device state.  The inputs (op records, layer ends, parameters, initial terms) sit in one
+  // device block, uploaded by one copy whenever a setter changed them.
   BInst* d_inst = nullptr;
   BInst* h_inst = nullptr;  // pinned mirror
+  void* d_input = nullptr;
+  size_t input_bytes = 0;   // capacity of d_input
   BOp* d_ops = nullptr;
   uint32_t* d_lends = nullptr;
+  double* d_params = nullptr;
+  uint64_t* d_init = nullptr;
   uint64_t* pool = nullptr;
   size_t pool_words = 0;
   double* d_out = nullptr;
-  bool ops_dirty = true;
+  bool inputs_dirty = true;
   bool layout_dirty = true;
   std::vector<cudaGraphExec_t> graphs;
   int graph_cfg[3] = {0, 0, 0};
@@ -605,8 +674,8 @@ int batch_words(uint32_t n_max) {
 
 template <int W, int BLOCK, int ITEMS>
 cudaError_t launch_layer(ppvm_batch* b, int layer) {
-  k_batch<W, BLOCK, ITEMS><<<(unsigned)b->ninst, BLOCK, 0, b->stream>>>(b->d_inst, b->d_ops, b->d_lends, layer,
-                                                                         b->pool);
+  k_batch<W, BLOCK, ITEMS><<<(unsigned)b->ninst, BLOCK, 0, b->stream>>>(b->d_inst, b->d_ops, b->d_lends,
+                                                                         b->d_params, layer, b->pool);
   return cudaGetLastError();
 }
 
@@ -637,8 +706,8 @@ void launch_relocate(ppvm_batch* b, const BInst* d_old, uint64_t* old_pool, uint
   k_batch_relocate<W><<<(unsigned)b->ninst, 256, 0, b->stream>>>(d_old, b->d_inst, old_pool, new_pool);
 }
 template <int W>
-void launch_load(ppvm_batch* b, const unsigned long long* d_off, const uint64_t* d_src) {
-  k_batch_load<W><<<(unsigned)b->ninst, 256, 0, b->stream>>>(b->d_inst, d_off, d_src, b->pool);
+void launch_load(ppvm_batch* b) {
+  k_batch_load<W><<<(unsigned)b->ninst, 256, 0, b->stream>>>(b->d_inst, b->d_init, b->pool);
 }
 template <int W>
 void launch_owz(ppvm_batch* b) {
@@ -652,35 +721,86 @@ void launch_owz(ppvm_batch* b) {
     default: FN<8>(__VA_ARGS__); break; \
   }
 
-ppvm_status upload_ops(ppvm_batch* b) {
-  if (!b->ops_dirty) return PPVM_OK;
-  std::vector<BOp> all;
-  std::vector<uint32_t> le;
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Uploads what the setters changed: every instance's op records, layer ends (rebased to the
+// concatenated op list), parameter table and initial terms (packed x[k][W], z[k][W], c[k]),
+// written into the pinned staging buffer and copied to the device input block at once.
+ppvm_status upload_inputs(ppvm_batch* b) {
+  if (!b->inputs_dirty) return PPVM_OK;
+  const int W = b->W;
+  size_t nops = 0, nle = 0, npar = 0, ninit = 0;
+  for (size_t i = 0; i < b->ninst; ++i) {
+    nops += b->ops[i].size();
+    nle += b->lends[i].size();
+    npar += b->params[i].size();
+    ninit += (size_t)(2 * W + 1) * b->ic[i].size();
+  }
+  if (nops >= 0xFFFFFFF0ull || nle >= 0xFFFFFFF0ull) return bfail(PPVM_ECAPACITY, "batch op list too long");
+  const size_t o_ops = 0, o_le = align256(sizeof(BOp) * nops), o_par = o_le + align256(sizeof(uint32_t) * nle),
+               o_init = o_par + align256(sizeof(double) * npar),
+               total = std::max<size_t>(o_init + align256(sizeof(uint64_t) * ninit), 256);
+  BCUDA(cudaStreamSynchronize(b->stream));  // the previous block may still be read
+  if (total > b->input_bytes) {
+    ppvm::cache_free(b->d_input);
+    b->d_input = nullptr;
+    b->input_bytes = 0;
+    BCUDA(ppvm::cache_malloc(&b->d_input, total));
+    b->input_bytes = total;
+  }
+  Staging& st = staging();
+  std::lock_guard<std::mutex> lk(st.mu);
+  if (st.cap < total) {
+    if (st.p) cudaFreeHost(st.p);
+    st.p = nullptr;
+    st.cap = 0;
+    const size_t want = std::max(total, (size_t)(1u << 20));
+    BCUDA(cudaMallocHost(&st.p, want));
+    st.cap = want;
+  }
+  char* h = static_cast<char*>(st.p);
+  BOp* h_ops = reinterpret_cast<BOp*>(h + o_ops);
+  uint32_t* h_le = reinterpret_cast<uint32_t*>(h + o_le);
+  double* h_par = reinterpret_cast<double*>(h + o_par);
+  uint64_t* h_init = reinterpret_cast<uint64_t*>(h + o_init);
+  size_t at_op = 0, at_le = 0, at_par = 0, at_init = 0;
   b->max_layers = 0;
   for (size_t i = 0; i < b->ninst; ++i) {
     BInst& I = b->h_inst[i];
-    I.op_begin = (uint32_t)all.size();
-    I.layer_off = (uint32_t)le.size();
-    for (uint32_t e : b->lends[i]) le.push_back(I.op_begin + e);
+    const auto& ops = b->ops[i];
+    I.op_begin = (uint32_t)at_op;
+    I.layer_off = (uint32_t)at_le;
     I.n_layers = (uint32_t)b->lends[i].size();
-    all.insert(all.end(), b->ops[i].begin(), b->ops[i].end());
-    I.op_end = (uint32_t)all.size();
+    I.param_off = at_par;
+    I.init_off = at_init;
+    if (!ops.empty()) std::memcpy(h_ops + at_op, ops.data(), sizeof(BOp) * ops.size());
+    for (uint32_t e : b->lends[i]) h_le[at_le++] = I.op_begin + e;
+    at_op += ops.size();
+    I.op_end = (uint32_t)at_op;
+    if (!b->params[i].empty()) std::memcpy(h_par + at_par, b->params[i].data(), sizeof(double) * b->params[i].size());
+    at_par += b->params[i].size();
+    const int wi = words_of(b->nq[i]);
+    const size_t k = b->ic[i].size();
+    uint64_t* s = h_init + at_init;
+    std::memset(s, 0, sizeof(uint64_t) * 2 * W * k);
+    for (size_t t = 0; t < k; ++t)
+      for (int w = 0; w < wi; ++w) {
+        s[t * W + w] = b->ix[i][t * wi + w];
+        s[k * W + t * W + w] = b->iz[i][t * wi + w];
+      }
+    if (k) std::memcpy(s + 2 * k * W, b->ic[i].data(), sizeof(double) * k);
+    at_init += (size_t)(2 * W + 1) * k;
     b->max_layers = std::max(b->max_layers, I.n_layers);
   }
-  if (all.size() >= 0xFFFFFFF0ull) return bfail(PPVM_ECAPACITY, "batch op list too long");
-  cudaFree(b->d_ops);
-  cudaFree(b->d_lends);
-  b->d_ops = nullptr;
-  b->d_lends = nullptr;
-  BCUDA(cudaMalloc(&b->d_ops, sizeof(BOp) * std::max<size_t>(all.size(), 1)));
-  BCUDA(cudaMalloc(&b->d_lends, sizeof(uint32_t) * std::max<size_t>(le.size(), 1)));
-  if (!all.empty())
-    BCUDA(cudaMemcpyAsync(b->d_ops, all.data(), sizeof(BOp) * all.size(), cudaMemcpyHostToDevice, b->stream));
-  b->xfer_h2d += sizeof(BOp) * all.size() + sizeof(uint32_t) * le.size();
-  if (!le.empty())
-    BCUDA(cudaMemcpyAsync(b->d_lends, le.data(), sizeof(uint32_t) * le.size(), cudaMemcpyHostToDevice, b->stream));
-  BCUDA(cudaStreamSynchronize(b->stream));
-  b->ops_dirty = false;
+  char* d = static_cast<char*>(b->d_input);
+  b->d_ops = reinterpret_cast<BOp*>(d + o_ops);
+  b->d_lends = reinterpret_cast<uint32_t*>(d + o_le);
+  b->d_params = reinterpret_cast<double*>(d + o_par);
+  b->d_init = reinterpret_cast<uint64_t*>(d + o_init);
+  BCUDA(cudaMemcpyAsync(b->d_input, st.p, total, cudaMemcpyHostToDevice, b->stream));
+  BCUDA(cudaStreamSynchronize(b->stream));  // the staging buffer is free again
+  b->xfer_h2d += total;
+  b->inputs_dirty = false;
   drop_graphs(b);
   return PPVM_OK;
 }
@@ -698,48 +818,47 @@ ppvm_status layout(ppvm_batch* b, bool keep) {
     words = (words + 31) & ~31ull;  // 256-byte aligned regions
     I.epoch = 0;
   }
-  uint64_t* np = nullptr;
-  BCUDA(cudaMalloc(&np, sizeof(uint64_t) * std::max<unsigned long long>(words, 1)));
-  BCUDA(cudaMemsetAsync(np, 0, sizeof(uint64_t) * std::max<unsigned long long>(words, 1), b->stream));
-  if (keep && b->pool) {
-    BInst* d_old = nullptr;
-    BCUDA(cudaMalloc(&d_old, sizeof(BInst) * b->ninst));
-    BCUDA(cudaMemcpyAsync(d_old, old.data(), sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
-    BCUDA(cudaMemcpyAsync(b->d_inst, b->h_inst, sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
-    b->xfer_h2d += 2 * sizeof(BInst) * b->ninst;
-    BDISPATCH(b->W, launch_relocate, b, d_old, b->pool, np);
-    BCUDA(cudaGetLastError());
-    BCUDA(cudaStreamSynchronize(b->stream));
-    cudaFree(d_old);
-  }
+  const size_t bytes = sizeof(uint64_t) * std::max<unsigned long long>(words, 1);
   BCUDA(cudaStreamSynchronize(b->stream));
-  cudaFree(b->pool);
-  b->pool = np;
+  void* np = nullptr;
+  BCUDA(ppvm::cache_malloc(&np, bytes));
+  // zeroed: pair-table slots of an earlier user must not carry a live epoch
+  cudaError_t e = cudaMemsetAsync(np, 0, bytes, b->stream);
+  void* d_old = nullptr;
+  if (e == cudaSuccess && keep && b->pool) {
+    e = ppvm::cache_malloc(&d_old, sizeof(BInst) * b->ninst);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_old, old.data(), sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(b->d_inst, b->h_inst, sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) {
+      b->xfer_h2d += 2 * sizeof(BInst) * b->ninst;
+      BDISPATCH(b->W, launch_relocate, b, static_cast<BInst*>(d_old), b->pool, static_cast<uint64_t*>(np));
+      e = cudaGetLastError();
+    }
+  }
+  const cudaError_t se = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = se;
+  ppvm::cache_free(d_old);
+  if (e != cudaSuccess) {
+    if (se == cudaSuccess) ppvm::cache_free(np);
+    return bfail(e == cudaErrorMemoryAllocation ? PPVM_ECAPACITY : PPVM_ECUDA,
+                 std::string("batch layout: ") + cudaGetErrorString(e));
+  }
+  ppvm::cache_free(b->pool);
+  b->pool = static_cast<uint64_t*>(np);
   b->pool_words = words;
   b->layout_dirty = false;
   drop_graphs(b);
   return PPVM_OK;
 }
 
-// Resets every instance to its initial terms (uploaded packed, scattered by a kernel).
+// Resets every instance to its initial terms (resident in the input block, scattered into
+// the regions by a kernel).
 ppvm_status load_initial(ppvm_batch* b) {
-  std::vector<unsigned long long> off(b->ninst);
-  std::vector<uint64_t> packed;
-  const int W = b->W;
   for (size_t i = 0; i < b->ninst; ++i) {
-    const int wi = words_of(b->nq[i]);
-    const size_t k = b->ic[i].size();
-    off[i] = packed.size();
-    const size_t at = packed.size();
-    packed.resize(at + (2 * W + 1) * k, 0);
-    for (size_t t = 0; t < k; ++t)
-      for (int w = 0; w < wi; ++w) {
-        packed[at + t * W + w] = b->ix[i][t * wi + w];
-        packed[at + k * W + t * W + w] = b->iz[i][t * wi + w];
-      }
-    if (k) std::memcpy(&packed[at + 2 * k * W], b->ic[i].data(), sizeof(double) * k);
     BInst& I = b->h_inst[i];
-    I.n = k;
+    I.n = b->ic[i].size();
     I.pc = I.op_begin;
     I.tgu = 0;
     I.need = 0;
@@ -747,20 +866,10 @@ ppvm_status load_initial(ppvm_batch* b) {
     I.thr = b->thr[i];
     I.maxw = b->maxw[i];
   }
-  uint64_t* d_src = nullptr;
-  unsigned long long* d_off = nullptr;
-  BCUDA(cudaMalloc(&d_src, sizeof(uint64_t) * std::max<size_t>(packed.size(), 1)));
-  BCUDA(cudaMalloc(&d_off, sizeof(unsigned long long) * b->ninst));
-  if (!packed.empty())
-    BCUDA(cudaMemcpyAsync(d_src, packed.data(), sizeof(uint64_t) * packed.size(), cudaMemcpyHostToDevice, b->stream));
-  BCUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(unsigned long long) * b->ninst, cudaMemcpyHostToDevice, b->stream));
   BCUDA(cudaMemcpyAsync(b->d_inst, b->h_inst, sizeof(BInst) * b->ninst, cudaMemcpyHostToDevice, b->stream));
-  b->xfer_h2d += sizeof(uint64_t) * packed.size() + sizeof(unsigned long long) * b->ninst + sizeof(BInst) * b->ninst;
-  BDISPATCH(b->W, launch_load, b, d_off, d_src);
+  b->xfer_h2d += sizeof(BInst) * b->ninst;
+  BDISPATCH(b->W, launch_load, b);
   BCUDA(cudaGetLastError());
-  BCUDA(cudaStreamSynchronize(b->stream));
-  cudaFree(d_src);
-  cudaFree(d_off);
   return PPVM_OK;
 }
 
@@ -813,7 +922,7 @@ ppvm_status grow_failed(ppvm_batch* b, uint32_t* first) {
 
 ppvm_status run_all(ppvm_batch* b, bool use_graphs, bool persistent) {
   BCUDA(cudaSetDevice(b->device));
-  BTRY(upload_ops(b));
+  BTRY(upload_inputs(b));
   if (b->layout_dirty || !b->pool) BTRY(layout(b, false));
   BTRY(load_initial(b));
   uint32_t first = 0;
@@ -841,6 +950,16 @@ ppvm_status run_all(ppvm_batch* b, bool use_graphs, bool persistent) {
 
 }  // namespace
 
+namespace ppvm {
+void release_batch_staging() {
+  Staging& st = staging();
+  std::lock_guard<std::mutex> lk(st.mu);
+  if (st.p) cudaFreeHost(st.p);
+  st.p = nullptr;
+  st.cap = 0;
+}
+}  // namespace ppvm
+
 extern "C" {
 
 ppvm_status ppvm_batch_destroy(ppvm_batch* b) {
@@ -848,12 +967,11 @@ ppvm_status ppvm_batch_destroy(ppvm_batch* b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graphs(b);
-  cudaFree(b->d_inst);
+  ppvm::cache_free(b->d_inst);
   cudaFreeHost(b->h_inst);
-  cudaFree(b->d_ops);
-  cudaFree(b->d_lends);
-  cudaFree(b->pool);
-  cudaFree(b->d_out);
+  ppvm::cache_free(b->d_input);
+  ppvm::cache_free(b->pool);
+  ppvm::cache_free(b->d_out);
   if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
   delete b;
   return PPVM_OK;
@@ -887,12 +1005,13 @@ ppvm_status ppvm_batch_create(ppvm_batch** out, size_t n_inst, const uint32_t* n
   b->iz.resize(n_inst);
   b->ic.resize(n_inst);
   b->ops.resize(n_inst);
+  b->params.resize(n_inst);
   b->lends.resize(n_inst);
   b->cap.assign(n_inst, 256);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&b->d_inst, sizeof(BInst) * n_inst) != cudaSuccess ||
+      ppvm::cache_malloc((void**)&b->d_inst, sizeof(BInst) * n_inst) != cudaSuccess ||
       cudaMallocHost(&b->h_inst, sizeof(BInst) * n_inst) != cudaSuccess ||
-      cudaMalloc(&b->d_out, sizeof(double) * n_inst) != cudaSuccess) {
+      ppvm::cache_malloc((void**)&b->d_out, sizeof(double) * n_inst) != cudaSuccess) {
     ppvm_batch_destroy(b);
     return bfail(PPVM_ECAPACITY, "device allocation failed");
   }
@@ -945,8 +1064,12 @@ ppvm_status ppvm_batch_add_terms(ppvm_batch* b, size_t inst, const uint64_t* x, 
       Cc.push_back(c[t]);
     }
   }
-  b->cap[inst] = std::max<unsigned long long>(b->cap[inst], 2 * Cc.size() + 64);
-  b->layout_dirty = true;
+  const unsigned long long want = 2 * Cc.size() + 64;
+  if (want > b->cap[inst]) {
+    b->cap[inst] = want;
+    b->layout_dirty = true;
+  }
+  b->inputs_dirty = true;
   return PPVM_OK;
 }
 
@@ -957,20 +1080,30 @@ ppvm_status ppvm_batch_set_ops(ppvm_batch* b, size_t inst, const ppvm_op* ops, s
   const double half_pi = 1.5707963267948966;
   std::vector<BOp> out;
   out.reserve(n_ops);
+  std::vector<double> par;
   std::vector<uint32_t> le;
   int truncs = 0;
   SinCosMemo trig;
+  // consecutive ops with the same values (bit for bit) share one parameter entry
+  double last[3] = {0.0, 0.0, 0.0};
+  int last_k = 0;
+  uint32_t last_at = 0;
+  auto put = [&](const double* v, int k) -> uint32_t {
+    if (last_k == k && std::memcmp(last, v, sizeof(double) * k) == 0) return last_at;
+    last_at = (uint32_t)par.size();
+    par.insert(par.end(), v, v + k);
+    std::memcpy(last, v, sizeof(double) * k);
+    last_k = k;
+    return last_at;
+  };
   for (size_t i = 0; i < n_ops; ++i) {
     const ppvm_op& op = ops[i];
     if (op.flags != 0 || op.code >= PPVM_OP_COUNT_) return bfail(PPVM_EINVAL, "bad op code or flags");
     if (op.code == PPVM_OP_LOSS_CHANNEL || op.code == PPVM_OP_RESET_LOSS_CHANNEL ||
         op.code == PPVM_OP_CORRELATED_LOSS_CHANNEL)
       return bfail(PPVM_EINVAL, "batched instances hold plain words: loss channels need a lossy PauliSum");
-    BOp bo;
-    std::memset(&bo, 0, sizeof(bo));
     if (op.code == PPVM_OP_TRUNCATE) {
-      bo.kind = B_TRUNC;
-      out.push_back(bo);
+      out.push_back(BOp{bop_header(B_TRUNC, 0, false, 0, 0, 0, 0), 0u});
       if (++truncs % 2 == 0) le.push_back((uint32_t)out.size());
       continue;
     }
@@ -979,60 +1112,60 @@ ppvm_status ppvm_batch_set_ops(ppvm_batch* b, size_t inst, const ppvm_op* ops, s
                      op.code == PPVM_OP_DEPOLARIZE2;
     if (op.q0 >= n || (two && (op.q1 >= n || op.q1 == op.q0)))
       return bfail(PPVM_EINVAL, "qubit index out of range (or a two-qubit op on one qubit)");
-    DevOp& d = bo.d;
-    d.w0 = (uint16_t)(op.q0 >> 6);
-    d.b0 = (uint16_t)(op.q0 & 63);
-    d.w1 = (uint16_t)((two ? op.q1 : op.q0) >> 6);
-    d.b1 = (uint16_t)((two ? op.q1 : op.q0) & 63);
-    d.two = two ? 1 : 0;
+    const uint32_t q0 = op.q0, q1 = two ? op.q1 : op.q0;
     const bool rot = op.code >= PPVM_OP_RX && op.code <= PPVM_OP_RZZ;
     if (rot) {
       const bool gx = op.code == PPVM_OP_RX || op.code == PPVM_OP_RY || op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY;
       const bool gz = op.code == PPVM_OP_RZ || op.code == PPVM_OP_RY || op.code == PPVM_OP_RZZ || op.code == PPVM_OP_RYY;
-      d.ax = (uint16_t)((gx ? 1 : 0) | ((gx && two) ? 2 : 0));
-      d.az = (uint16_t)((gz ? 1 : 0) | ((gz && two) ? 2 : 0));
+      const uint32_t ax = (gx ? 1u : 0u) | ((gx && two) ? 2u : 0u);
+      const uint32_t az = (gz ? 1u : 0u) | ((gz && two) ? 2u : 0u);
       if ((b->flags & PPVM_FLAG_CLIFFORD_ANGLES) && (op.theta == half_pi || op.theta == -half_pi)) {
-        bo.kind = B_LOCAL;
-        d.code = C_ROTC;
-        d.f0 = op.theta > 0 ? 1.0 : -1.0;
+        const double sign = op.theta > 0 ? 1.0 : -1.0;
+        out.push_back(BOp{bop_header(B_LOCAL, C_ROTC, two, ax, az, q0, q1), put(&sign, 1)});
       } else {
-        bo.kind = B_ROT;
-        trig.get(op.theta, bo.sn, bo.cs);
+        double sc[2];
+        trig.get(op.theta, sc[0], sc[1]);
+        out.push_back(BOp{bop_header(B_ROT, 0, two, ax, az, q0, q1), put(sc, 2)});
       }
-    } else {
-      bo.kind = B_LOCAL;
-      switch (op.code) {
-        case PPVM_OP_X: d.code = C_X; break;
-        case PPVM_OP_Y: d.code = C_Y; break;
-        case PPVM_OP_Z: d.code = C_Z; break;
-        case PPVM_OP_H: d.code = C_H; break;
-        case PPVM_OP_S: d.code = C_S; break;
-        case PPVM_OP_S_DAG: d.code = C_SDAG; break;
-        case PPVM_OP_SQRT_X: d.code = C_SQX; break;
-        case PPVM_OP_SQRT_X_DAG: d.code = C_SQXDAG; break;
-        case PPVM_OP_SQRT_Y: d.code = C_SQY; break;
-        case PPVM_OP_SQRT_Y_DAG: d.code = C_SQYDAG; break;
-        case PPVM_OP_CNOT: d.code = C_CNOT; break;
-        case PPVM_OP_CZ: d.code = C_CZ; break;
-        case PPVM_OP_CY: d.code = C_CY; break;
-        case PPVM_OP_PAULI_ERROR: {  // noise.rs:17-37, factors as the per-op pass computes them
-          d.code = C_PAULI_ERROR;
-          const double one = 1.0;
-          d.f0 = one - op.p[1] * 2.0 - op.p[2] * 2.0;
-          d.f1 = one - op.p[0] * 2.0 - op.p[1] * 2.0;
-          d.f2 = one - op.p[0] * 2.0 - op.p[2] * 2.0;
-          break;
-        }
-        case PPVM_OP_DEPOLARIZE1: d.code = C_DEP1; d.f0 = 1.0 - op.theta * (4.0 / 3.0); break;
-        case PPVM_OP_DEPOLARIZE2: d.code = C_DEP2; d.f0 = 1.0 - op.theta * (16.0 / 15.0); break;
-        default: return bfail(PPVM_EINVAL, "unsupported op in a batch");
-      }
+      continue;
     }
-    out.push_back(bo);
+    uint32_t code = 0;
+    double f[3] = {0.0, 0.0, 0.0};
+    int nf = 0;
+    switch (op.code) {
+      case PPVM_OP_X: code = C_X; break;
+      case PPVM_OP_Y: code = C_Y; break;
+      case PPVM_OP_Z: code = C_Z; break;
+      case PPVM_OP_H: code = C_H; break;
+      case PPVM_OP_S: code = C_S; break;
+      case PPVM_OP_S_DAG: code = C_SDAG; break;
+      case PPVM_OP_SQRT_X: code = C_SQX; break;
+      case PPVM_OP_SQRT_X_DAG: code = C_SQXDAG; break;
+      case PPVM_OP_SQRT_Y: code = C_SQY; break;
+      case PPVM_OP_SQRT_Y_DAG: code = C_SQYDAG; break;
+      case PPVM_OP_CNOT: code = C_CNOT; break;
+      case PPVM_OP_CZ: code = C_CZ; break;
+      case PPVM_OP_CY: code = C_CY; break;
+      case PPVM_OP_PAULI_ERROR: {  // noise.rs:17-37, factors as the per-op pass computes them
+        code = C_PAULI_ERROR;
+        const double one = 1.0;
+        f[0] = one - op.p[1] * 2.0 - op.p[2] * 2.0;
+        f[1] = one - op.p[0] * 2.0 - op.p[1] * 2.0;
+        f[2] = one - op.p[0] * 2.0 - op.p[2] * 2.0;
+        nf = 3;
+        break;
+      }
+      case PPVM_OP_DEPOLARIZE1: code = C_DEP1; f[0] = 1.0 - op.theta * (4.0 / 3.0); nf = 1; break;
+      case PPVM_OP_DEPOLARIZE2: code = C_DEP2; f[0] = 1.0 - op.theta * (16.0 / 15.0); nf = 1; break;
+      default: return bfail(PPVM_EINVAL, "unsupported op in a batch");
+    }
+    out.push_back(BOp{bop_header(B_LOCAL, code, two, 0, 0, q0, q1), nf ? put(f, nf) : 0u});
   }
+  if (par.size() >= 0xFFFFFFF0ull) return bfail(PPVM_ECAPACITY, "batch parameter table too long");
   b->ops[inst] = std::move(out);
+  b->params[inst] = std::move(par);
   b->lends[inst] = std::move(le);
-  b->ops_dirty = true;
+  b->inputs_dirty = true;
   return PPVM_OK;
 }
 
@@ -1079,7 +1212,7 @@ ppvm_status ppvm_batch_run(ppvm_batch* b) {
   // Layer graphs pay off from the second run of an unchanged batch on.  A batch's first run
   // (and the first after new ops or a new layout) launches the layers directly, which saves
   // capturing and instantiating one graph per layer for a batch that runs once.
-  const bool reuse = b->ran && !b->ops_dirty && !b->layout_dirty;
+  const bool reuse = b->ran && !b->inputs_dirty && !b->layout_dirty;
   return run_all(b, reuse, false);
 }
 

@@ -1657,6 +1657,14 @@ ppvm_sum* take_cached(int device, int W) {
 }
 }  // namespace
 
+namespace ppvm {
+// The buffer cache for the other translation units (batch.cu): same rules as for the sums,
+// a buffer goes back only when the stream that used it is idle.
+cudaError_t cache_malloc(void** out, size_t bytes) { return pool_malloc(out, bytes); }
+void cache_free(void* p) { pool_free(p); }
+void release_batch_staging();  // batch.cu: frees the pinned staging buffer of the uploads
+}  // namespace ppvm
+
 extern "C" {
 
 ppvm_status ppvm_sum_destroy(ppvm_sum* s) {
@@ -2316,6 +2324,7 @@ ppvm_status ppvm_release_cached_memory(void) {
     handles.swap(g_sum_cache);
   }
   for (ppvm_sum* h : handles) destroy_now(h);  // their buffers go back to the pool first
+  ppvm::release_batch_staging();
   std::lock_guard<std::mutex> lk(g_pool_mu);
   for (int d = 0; d < 64; ++d) {
     if (g_pool_free[d].empty()) continue;

@@ -92,27 +92,27 @@ def words(n_qubits: int) -> int:
     return (n_qubits + 63) // 64
 
 
+_XBITS = str.maketrans("IXYZ", "0110")
+_ZBITS = str.maketrans("IXYZ", "0011")
+_M64 = (1 << 64) - 1
+
+
 def parse_word(s: str, n_qubits: int | None = None):
     """Pauli string -> (x[W], z[W]) u64 planes; '_' is skipped like the reference parser
     (crates/ppvm-pauli-word/src/word/data.rs:332-377)."""
-    chars = [c for c in s if c != "_"]
-    n = len(chars) if n_qubits is None else n_qubits
-    if len(chars) != n:
-        raise ValueError(f"word {s!r} has {len(chars)} qubits, expected {n}")
+    t = s.replace("_", "")
+    n = len(t) if n_qubits is None else n_qubits
+    if len(t) != n:
+        raise ValueError(f"word {s!r} has {len(t)} qubits, expected {n}")
+    if t.strip("IXYZ"):  # non-empty exactly when some character is not a Pauli letter
+        bad = next(c for c in t if c not in "IXYZ")
+        raise ValueError(f"Invalid Pauli character: {bad}")
     W = words(n)
-    x = np.zeros(W, dtype=np.uint64)
-    z = np.zeros(W, dtype=np.uint64)
-    for q, c in enumerate(chars):
-        b = np.uint64(1) << np.uint64(q % 64)
-        if c == "X":
-            x[q // 64] |= b
-        elif c == "Z":
-            z[q // 64] |= b
-        elif c == "Y":
-            x[q // 64] |= b
-            z[q // 64] |= b
-        elif c != "I":
-            raise ValueError(f"Invalid Pauli character: {c}")
+    # character q is bit q: reversed, the 0/1 string reads as a binary number
+    xv = int(t.translate(_XBITS)[::-1] or "0", 2)
+    zv = int(t.translate(_ZBITS)[::-1] or "0", 2)
+    x = np.array([(xv >> (64 * w)) & _M64 for w in range(W)], dtype=np.uint64)
+    z = np.array([(zv >> (64 * w)) & _M64 for w in range(W)], dtype=np.uint64)
     return x, z
 
 

@@ -108,3 +108,52 @@ def test_rejects_bad_instances():
         PauliSumBatch([Instance(4, [("ZIII", 1.0)], [G.g1(G.H, 4)])])
     with pytest.raises(ValueError):
         PauliSumBatch([Instance(4, [("ZIII", 1.0)], [G.g2(G.CNOT, 1, 1)])])
+
+
+def test_noise_parameters_and_replaced_instances():
+    # depolarising channels and repeated equal-valued ops (which share parameter entries),
+    # then the same batch with one instance's list and terms replaced: its inputs are
+    # uploaded again into the existing device block, and a later batch reuses the cached
+    # buffers of this one
+    rng = np.random.default_rng(21)
+    n = 9
+    hot = list(range(n))
+    ops = []
+    for i in range(60):
+        q = int(rng.integers(n))
+        k = i % 5
+        if k == 0:
+            ops.append(G.depolarize1(q, 0.01))
+        elif k == 1:
+            a, c = (int(v) for v in rng.choice(n, 2, replace=False))
+            ops.append(G.depolarize2(a, c, 0.02))
+        elif k == 2:
+            ops.append(G.r1(G.RX, q, 0.4))
+        elif k == 3:
+            ops.append(G.pauli_error(q, (0.01, 0.02, 0.03)))
+        else:
+            ops.append(G.r2(G.RZZ, q, (q + 1) % n, -0.7))
+        if i % 3 == 2:
+            ops.append(G.truncate())
+    insts = [Instance(n, [("Z" * n, 1.0), ("X" + "I" * (n - 1), 0.5)], ops, 1e-7, None),
+             Instance(12, [("Z" + "I" * 11, 1.0)], _random_ops(rng, 12, 80, hot), 1e-6, 6)]
+    b = PauliSumBatch(insts)
+    b.run()
+    check_batch(b)
+    b.run()  # unchanged: replayed layer graphs
+    check_batch(b)
+    from ppvm_b200._lib import lib
+    from ppvm_b200.paulisum import _p64, _pd, ops_array
+    new_ops = _random_ops(rng, 12, 40, hot)
+    gl = ops_array(new_ops)
+    b._check(lib().ppvm_batch_set_ops(b._h, 1, gl.ptr, len(gl)))
+    x, z = G.parse_word("IZ" + "I" * 10, 12)
+    c = np.array([1.0])
+    b._check(lib().ppvm_batch_add_terms(b._h, 1, _p64(x), _p64(z), _pd(c), 1))  # += into the terms
+    b.instances[1] = Instance(12, [("Z" + "I" * 11, 1.0), ("IZ" + "I" * 10, 1.0)], new_ops, 1e-6, 6)
+    b.run()
+    check_batch(b)
+    del b
+    b2 = PauliSumBatch(insts)
+    b2.run()
+    check_batch(b2)
