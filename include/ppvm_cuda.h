@@ -310,6 +310,10 @@ ppvm_status ppvm_batch_add_terms(ppvm_batch* batch, size_t inst, const uint64_t*
                                  const uint64_t* z, const double* c, size_t k);
 /* Gate list of instance `inst` (as ppvm_gate_list_run takes it). */
 ppvm_status ppvm_batch_set_ops(ppvm_batch* batch, size_t inst, const ppvm_op* ops, size_t n_ops);
+/* Gate lists of every instance at once (ops[i], n_ops[i] for instance i; n_inst of each),
+ * packed by several host threads.  All or nothing: on a bad list no instance changes and the
+ * error names the first failing instance. */
+ppvm_status ppvm_batch_set_ops_all(ppvm_batch* batch, const ppvm_op* const* ops, const size_t* n_ops);
 /* Runs every instance from its initial terms through its whole list.  Inputs changed by
  * the setters since the last run (8-byte op records, parameter tables, initial terms) go to
  * the device in one copy from a pinned staging buffer; the first run of a batch launches the

@@ -101,6 +101,7 @@ _SIGS = {
     "ppvm_batch_set_stream": [_P, _P],
     "ppvm_batch_add_terms": [_P, _SZ, _U64P, _U64P, _DP, _SZ],
     "ppvm_batch_set_ops": [_P, _SZ, ctypes.POINTER(Op), _SZ],
+    "ppvm_batch_set_ops_all": [_P, ctypes.POINTER(ctypes.POINTER(Op)), _SZP],
     "ppvm_batch_run": [_P],
     "ppvm_batch_run_persistent": [_P],
     "ppvm_batch_reserve": [_P, _U64P],

@@ -17,7 +17,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import gates as G
-from ._lib import EINVAL, FLAG_CLIFFORD_ANGLES, OK, UMAX, PPVMError, lib
+from ._lib import EINVAL, FLAG_CLIFFORD_ANGLES, OK, UMAX, Op, PPVMError, lib
 from .paulisum import GateList, _p64, _pd, ops_array
 
 
@@ -46,6 +46,7 @@ class PauliSumBatch:
                                             FLAG_CLIFFORD_ANGLES if clifford_angles else 0, device))
         self._h = h
         self.instances = instances
+        lists = []
         for j, inst in enumerate(instances):
             if inst.terms:
                 W = G.words(inst.n_qubits)
@@ -55,8 +56,11 @@ class PauliSumBatch:
                     x[t], z[t] = G.parse_word(w, inst.n_qubits)
                 c = np.array([float(cf) for _, cf in inst.terms], dtype=np.float64)
                 self._check(lib().ppvm_batch_add_terms(self._h, j, _p64(x), _p64(z), _pd(c), len(c)))
-            gl = inst.ops if isinstance(inst.ops, GateList) else ops_array(inst.ops)
-            self._check(lib().ppvm_batch_set_ops(self._h, j, gl.ptr, len(gl)))
+            lists.append(inst.ops if isinstance(inst.ops, GateList) else ops_array(inst.ops))
+        # every list in one call: the library packs them on several host threads
+        ptrs = (ctypes.POINTER(Op) * k)(*[gl.ptr for gl in lists])
+        counts = (ctypes.c_size_t * k)(*[len(gl) for gl in lists])
+        self._check(lib().ppvm_batch_set_ops_all(self._h, ptrs, counts))
         if capacity is not None:
             caps = np.ascontiguousarray(capacity, dtype=np.uint64)
             if caps.shape != (k,):

@@ -30,7 +30,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -950,6 +952,117 @@ ppvm_status run_all(ppvm_batch* b, bool use_graphs, bool persistent) {
 
 }  // namespace
 
+namespace {
+
+// One instance's gate list as op records, parameter table and layer ends.  Runs on any host
+// thread: a failure is returned with its message instead of being recorded.
+struct Packed {
+  std::vector<BOp> out;
+  std::vector<double> par;
+  std::vector<uint32_t> le;
+  ppvm_status st = PPVM_OK;
+  const char* msg = nullptr;
+  ppvm_status fail(ppvm_status s, const char* m) {
+    st = s;
+    msg = m;
+    return s;
+  }
+};
+
+ppvm_status pack_ops(uint32_t n, uint32_t flags, const ppvm_op* ops, size_t n_ops, Packed& pk) {
+  const double half_pi = 1.5707963267948966;
+  std::vector<BOp>& out = pk.out;
+  std::vector<double>& par = pk.par;
+  std::vector<uint32_t>& le = pk.le;
+  out.clear();
+  par.clear();
+  le.clear();
+  out.reserve(n_ops);
+  int truncs = 0;
+  SinCosMemo trig;
+  // consecutive ops with the same values (bit for bit) share one parameter entry
+  double last[3] = {0.0, 0.0, 0.0};
+  int last_k = 0;
+  uint32_t last_at = 0;
+  auto put = [&](const double* v, int k) -> uint32_t {
+    if (last_k == k && std::memcmp(last, v, sizeof(double) * k) == 0) return last_at;
+    last_at = (uint32_t)par.size();
+    par.insert(par.end(), v, v + k);
+    std::memcpy(last, v, sizeof(double) * k);
+    last_k = k;
+    return last_at;
+  };
+  for (size_t i = 0; i < n_ops; ++i) {
+    const ppvm_op& op = ops[i];
+    if (op.flags != 0 || op.code >= PPVM_OP_COUNT_) return pk.fail(PPVM_EINVAL, "bad op code or flags");
+    if (op.code == PPVM_OP_LOSS_CHANNEL || op.code == PPVM_OP_RESET_LOSS_CHANNEL ||
+        op.code == PPVM_OP_CORRELATED_LOSS_CHANNEL)
+      return pk.fail(PPVM_EINVAL, "batched instances hold plain words: loss channels need a lossy PauliSum");
+    if (op.code == PPVM_OP_TRUNCATE) {
+      out.push_back(BOp{bop_header(B_TRUNC, 0, false, 0, 0, 0, 0), 0u});
+      if (++truncs % 2 == 0) le.push_back((uint32_t)out.size());
+      continue;
+    }
+    const bool two = op.code == PPVM_OP_CNOT || op.code == PPVM_OP_CZ || op.code == PPVM_OP_CY ||
+                     op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY || op.code == PPVM_OP_RZZ ||
+                     op.code == PPVM_OP_DEPOLARIZE2;
+    if (op.q0 >= n || (two && (op.q1 >= n || op.q1 == op.q0)))
+      return pk.fail(PPVM_EINVAL, "qubit index out of range (or a two-qubit op on one qubit)");
+    const uint32_t q0 = op.q0, q1 = two ? op.q1 : op.q0;
+    const bool rot = op.code >= PPVM_OP_RX && op.code <= PPVM_OP_RZZ;
+    if (rot) {
+      const bool gx = op.code == PPVM_OP_RX || op.code == PPVM_OP_RY || op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY;
+      const bool gz = op.code == PPVM_OP_RZ || op.code == PPVM_OP_RY || op.code == PPVM_OP_RZZ || op.code == PPVM_OP_RYY;
+      const uint32_t ax = (gx ? 1u : 0u) | ((gx && two) ? 2u : 0u);
+      const uint32_t az = (gz ? 1u : 0u) | ((gz && two) ? 2u : 0u);
+      if ((flags & PPVM_FLAG_CLIFFORD_ANGLES) && (op.theta == half_pi || op.theta == -half_pi)) {
+        const double sign = op.theta > 0 ? 1.0 : -1.0;
+        out.push_back(BOp{bop_header(B_LOCAL, C_ROTC, two, ax, az, q0, q1), put(&sign, 1)});
+      } else {
+        double sc[2];
+        trig.get(op.theta, sc[0], sc[1]);
+        out.push_back(BOp{bop_header(B_ROT, 0, two, ax, az, q0, q1), put(sc, 2)});
+      }
+      continue;
+    }
+    uint32_t code = 0;
+    double f[3] = {0.0, 0.0, 0.0};
+    int nf = 0;
+    switch (op.code) {
+      case PPVM_OP_X: code = C_X; break;
+      case PPVM_OP_Y: code = C_Y; break;
+      case PPVM_OP_Z: code = C_Z; break;
+      case PPVM_OP_H: code = C_H; break;
+      case PPVM_OP_S: code = C_S; break;
+      case PPVM_OP_S_DAG: code = C_SDAG; break;
+      case PPVM_OP_SQRT_X: code = C_SQX; break;
+      case PPVM_OP_SQRT_X_DAG: code = C_SQXDAG; break;
+      case PPVM_OP_SQRT_Y: code = C_SQY; break;
+      case PPVM_OP_SQRT_Y_DAG: code = C_SQYDAG; break;
+      case PPVM_OP_CNOT: code = C_CNOT; break;
+      case PPVM_OP_CZ: code = C_CZ; break;
+      case PPVM_OP_CY: code = C_CY; break;
+      case PPVM_OP_PAULI_ERROR: {  // noise.rs:17-37, factors as the per-op pass computes them
+        code = C_PAULI_ERROR;
+        const double one = 1.0;
+        f[0] = one - op.p[1] * 2.0 - op.p[2] * 2.0;
+        f[1] = one - op.p[0] * 2.0 - op.p[1] * 2.0;
+        f[2] = one - op.p[0] * 2.0 - op.p[2] * 2.0;
+        nf = 3;
+        break;
+      }
+      case PPVM_OP_DEPOLARIZE1: code = C_DEP1; f[0] = 1.0 - op.theta * (4.0 / 3.0); nf = 1; break;
+      case PPVM_OP_DEPOLARIZE2: code = C_DEP2; f[0] = 1.0 - op.theta * (16.0 / 15.0); nf = 1; break;
+      default: return pk.fail(PPVM_EINVAL, "unsupported op in a batch");
+    }
+    out.push_back(BOp{bop_header(B_LOCAL, code, two, 0, 0, q0, q1), nf ? put(f, nf) : 0u});
+  }
+  if (par.size() >= 0xFFFFFFF0ull) return pk.fail(PPVM_ECAPACITY, "batch parameter table too long");
+  return PPVM_OK;
+}
+
+}  // namespace
+
 namespace ppvm {
 void release_batch_staging() {
   Staging& st = staging();
@@ -1076,95 +1189,40 @@ ppvm_status ppvm_batch_add_terms(ppvm_batch* b, size_t inst, const uint64_t* x, 
 ppvm_status ppvm_batch_set_ops(ppvm_batch* b, size_t inst, const ppvm_op* ops, size_t n_ops) {
   if (!b || inst >= b->ninst) return bfail(PPVM_EINVAL, "bad batch or instance index");
   if (n_ops && !ops) return bfail(PPVM_EINVAL, "null op list");
-  const uint32_t n = b->nq[inst];
-  const double half_pi = 1.5707963267948966;
-  std::vector<BOp> out;
-  out.reserve(n_ops);
-  std::vector<double> par;
-  std::vector<uint32_t> le;
-  int truncs = 0;
-  SinCosMemo trig;
-  // consecutive ops with the same values (bit for bit) share one parameter entry
-  double last[3] = {0.0, 0.0, 0.0};
-  int last_k = 0;
-  uint32_t last_at = 0;
-  auto put = [&](const double* v, int k) -> uint32_t {
-    if (last_k == k && std::memcmp(last, v, sizeof(double) * k) == 0) return last_at;
-    last_at = (uint32_t)par.size();
-    par.insert(par.end(), v, v + k);
-    std::memcpy(last, v, sizeof(double) * k);
-    last_k = k;
-    return last_at;
+  Packed pk;
+  if (pack_ops(b->nq[inst], b->flags, ops, n_ops, pk) != PPVM_OK) return bfail(pk.st, pk.msg);
+  b->ops[inst] = std::move(pk.out);
+  b->params[inst] = std::move(pk.par);
+  b->lends[inst] = std::move(pk.le);
+  b->inputs_dirty = true;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_batch_set_ops_all(ppvm_batch* b, const ppvm_op* const* ops, const size_t* n_ops) {
+  if (!b || !ops || !n_ops) return bfail(PPVM_EINVAL, "null argument");
+  for (size_t i = 0; i < b->ninst; ++i)
+    if (n_ops[i] && !ops[i]) return bfail(PPVM_EINVAL, "null op list of instance " + std::to_string(i));
+  std::vector<Packed> pk(b->ninst);
+  size_t total = 0;
+  for (size_t i = 0; i < b->ninst; ++i) total += n_ops[i];
+  // host threads over instances, each packing whole lists (about 10^5 ops per thread at least)
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min({hw, (size_t)16, b->ninst, total / 100000 + 1});
+  std::atomic<size_t> next{0};
+  auto work = [&] {
+    for (size_t i; (i = next.fetch_add(1)) < b->ninst;) pack_ops(b->nq[i], b->flags, ops[i], n_ops[i], pk[i]);
   };
-  for (size_t i = 0; i < n_ops; ++i) {
-    const ppvm_op& op = ops[i];
-    if (op.flags != 0 || op.code >= PPVM_OP_COUNT_) return bfail(PPVM_EINVAL, "bad op code or flags");
-    if (op.code == PPVM_OP_LOSS_CHANNEL || op.code == PPVM_OP_RESET_LOSS_CHANNEL ||
-        op.code == PPVM_OP_CORRELATED_LOSS_CHANNEL)
-      return bfail(PPVM_EINVAL, "batched instances hold plain words: loss channels need a lossy PauliSum");
-    if (op.code == PPVM_OP_TRUNCATE) {
-      out.push_back(BOp{bop_header(B_TRUNC, 0, false, 0, 0, 0, 0), 0u});
-      if (++truncs % 2 == 0) le.push_back((uint32_t)out.size());
-      continue;
-    }
-    const bool two = op.code == PPVM_OP_CNOT || op.code == PPVM_OP_CZ || op.code == PPVM_OP_CY ||
-                     op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY || op.code == PPVM_OP_RZZ ||
-                     op.code == PPVM_OP_DEPOLARIZE2;
-    if (op.q0 >= n || (two && (op.q1 >= n || op.q1 == op.q0)))
-      return bfail(PPVM_EINVAL, "qubit index out of range (or a two-qubit op on one qubit)");
-    const uint32_t q0 = op.q0, q1 = two ? op.q1 : op.q0;
-    const bool rot = op.code >= PPVM_OP_RX && op.code <= PPVM_OP_RZZ;
-    if (rot) {
-      const bool gx = op.code == PPVM_OP_RX || op.code == PPVM_OP_RY || op.code == PPVM_OP_RXX || op.code == PPVM_OP_RYY;
-      const bool gz = op.code == PPVM_OP_RZ || op.code == PPVM_OP_RY || op.code == PPVM_OP_RZZ || op.code == PPVM_OP_RYY;
-      const uint32_t ax = (gx ? 1u : 0u) | ((gx && two) ? 2u : 0u);
-      const uint32_t az = (gz ? 1u : 0u) | ((gz && two) ? 2u : 0u);
-      if ((b->flags & PPVM_FLAG_CLIFFORD_ANGLES) && (op.theta == half_pi || op.theta == -half_pi)) {
-        const double sign = op.theta > 0 ? 1.0 : -1.0;
-        out.push_back(BOp{bop_header(B_LOCAL, C_ROTC, two, ax, az, q0, q1), put(&sign, 1)});
-      } else {
-        double sc[2];
-        trig.get(op.theta, sc[0], sc[1]);
-        out.push_back(BOp{bop_header(B_ROT, 0, two, ax, az, q0, q1), put(sc, 2)});
-      }
-      continue;
-    }
-    uint32_t code = 0;
-    double f[3] = {0.0, 0.0, 0.0};
-    int nf = 0;
-    switch (op.code) {
-      case PPVM_OP_X: code = C_X; break;
-      case PPVM_OP_Y: code = C_Y; break;
-      case PPVM_OP_Z: code = C_Z; break;
-      case PPVM_OP_H: code = C_H; break;
-      case PPVM_OP_S: code = C_S; break;
-      case PPVM_OP_S_DAG: code = C_SDAG; break;
-      case PPVM_OP_SQRT_X: code = C_SQX; break;
-      case PPVM_OP_SQRT_X_DAG: code = C_SQXDAG; break;
-      case PPVM_OP_SQRT_Y: code = C_SQY; break;
-      case PPVM_OP_SQRT_Y_DAG: code = C_SQYDAG; break;
-      case PPVM_OP_CNOT: code = C_CNOT; break;
-      case PPVM_OP_CZ: code = C_CZ; break;
-      case PPVM_OP_CY: code = C_CY; break;
-      case PPVM_OP_PAULI_ERROR: {  // noise.rs:17-37, factors as the per-op pass computes them
-        code = C_PAULI_ERROR;
-        const double one = 1.0;
-        f[0] = one - op.p[1] * 2.0 - op.p[2] * 2.0;
-        f[1] = one - op.p[0] * 2.0 - op.p[1] * 2.0;
-        f[2] = one - op.p[0] * 2.0 - op.p[2] * 2.0;
-        nf = 3;
-        break;
-      }
-      case PPVM_OP_DEPOLARIZE1: code = C_DEP1; f[0] = 1.0 - op.theta * (4.0 / 3.0); nf = 1; break;
-      case PPVM_OP_DEPOLARIZE2: code = C_DEP2; f[0] = 1.0 - op.theta * (16.0 / 15.0); nf = 1; break;
-      default: return bfail(PPVM_EINVAL, "unsupported op in a batch");
-    }
-    out.push_back(BOp{bop_header(B_LOCAL, code, two, 0, 0, q0, q1), nf ? put(f, nf) : 0u});
+  std::vector<std::thread> th;
+  for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+  for (size_t i = 0; i < b->ninst; ++i)  // nothing changes unless every list is valid
+    if (pk[i].st != PPVM_OK) return bfail(pk[i].st, "instance " + std::to_string(i) + ": " + pk[i].msg);
+  for (size_t i = 0; i < b->ninst; ++i) {
+    b->ops[i] = std::move(pk[i].out);
+    b->params[i] = std::move(pk[i].par);
+    b->lends[i] = std::move(pk[i].le);
   }
-  if (par.size() >= 0xFFFFFFF0ull) return bfail(PPVM_ECAPACITY, "batch parameter table too long");
-  b->ops[inst] = std::move(out);
-  b->params[inst] = std::move(par);
-  b->lends[inst] = std::move(le);
   b->inputs_dirty = true;
   return PPVM_OK;
 }

@@ -157,3 +157,13 @@ def test_noise_parameters_and_replaced_instances():
     b2 = PauliSumBatch(insts)
     b2.run()
     check_batch(b2)
+
+
+def test_bulk_setter_names_the_failing_instance():
+    good = Instance(4, [("ZIII", 1.0)], [G.r1(G.RX, 0, 0.3), G.truncate()])
+    bad = Instance(4, [("ZIII", 1.0)], [G.g1(G.H, 0), G.amplitude_damping(1, 0.1)])
+    with pytest.raises(ValueError, match="instance 1"):
+        PauliSumBatch([good, bad, good])
+    b = PauliSumBatch([good, good])
+    b.run()
+    check_batch(b)
