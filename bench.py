@@ -59,18 +59,22 @@ def parse():
     ap.add_argument("--impl", default="ppvm_b200", choices=["ppvm_b200", "reference"])
     ap.add_argument("--layers", type=int, default=20, help="kicked_ising_2d: layers of the circuit")
     ap.add_argument("--workload", default="kicked_ising_2d",
-                    choices=[*SINGLE_SUM, "batched_tfim", "learned_kicked_ising", "layer_bandwidth"],
+                    choices=[*SINGLE_SUM, "batched_tfim", "learned_kicked_ising", "layer_bandwidth",
+                             "kernel_families"],
                     help="kicked_ising_2d: one 12x12 sum (headline); tfim_1d: one 20-qubit TFIM chain; "
                          "clifford_t: the first 26 layers of the n=64 Clifford+T brickwork; "
                          "batched_tfim: 256 independent 1D TFIM "
                          "instances through the batched engine; learned_kicked_ising: time to <O> within 1e-3 "
                          "with learned vs plain term-budget truncation on a 10x10 kicked-Ising circuit; "
                          "layer_bandwidth: the 12x12 circuit at --thr/--max-weight, one line per layer with "
-                         "each kernel family's time and algorithmic bandwidth (sums larger than L2)")
+                         "each kernel family's time and algorithmic bandwidth (sums larger than L2); "
+                         "kernel_families: one op per kernel family on a copy of a sum larger than L2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--thr", type=float, default=1e-7, help="layer_bandwidth: coefficient threshold")
     ap.add_argument("--max-weight", type=int, default=12, help="layer_bandwidth: weight cap")
     ap.add_argument("--stop-terms", type=float, default=4e7, help="layer_bandwidth: stop past this many terms")
+    ap.add_argument("--family-terms", type=float, default=3e6,
+                    help="kernel_families: grow the sums past this many terms")
     return ap.parse_args()
 
 
@@ -803,10 +807,93 @@ def run_layer_bandwidth(args):
             break
 
 
+def run_kernel_families(args):
+    """Every kernel family of the single-sum engine, one op at a time, on sums larger than L2.
+
+    The 12x12 kicked-Ising circuit at --thr / --max-weight is propagated until the sum holds
+    more than --family-terms terms, three times: in the reference's term order (per-gate
+    rotation path), as a lossy sum (loss channels) and as a term set (fused runs).  Each op
+    below then runs on a fresh device copy of that sum, after an L2 flush, with the per-op
+    profile on: per kernel family the launches, CUDA-event time, algorithmic bytes (the
+    engine's per-op log) and their rate against the measured copy bandwidth.  Each op sits in
+    an NVTX range "kf:<op>", so that an ncu capture can select exactly its launches.  One
+    JSON line per op; not a bench line."""
+    import torch
+
+    from ppvm_b200 import gates as G
+    from ppvm_b200 import learned
+    from ppvm_b200.paulisum import LossyPauliSum, PauliSum, ops_array
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    peak, peak_kind = measured_peak()
+    wl = C.kicked_ising_2d(L=12, layers=20, theta_h=0.6, thr=args.thr, max_weight=args.max_weight)
+    lay = [ops_array(p) for p in learned.split_layers(wl.ops)]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def grown(cls, exact):
+        s = cls([wl.observable[0][0]], wl.n_qubits, [1.0], min_abs_coeff=args.thr,
+                max_pauli_weight=args.max_weight, clifford_angles=True, exact_order=exact, capacity=1 << 22)
+        for a in lay:
+            if len(s) > args.family_terms:
+                break
+            s.run(a)
+        return s
+
+    n = wl.n_qubits
+    rzz_layer = [op for op in wl.ops if op[0] == G.RZZ][:264]  # the 264 RZZ(-pi/2) bonds of one layer
+    cases = [
+        ("exact", "rx", [G.r1(G.RX, 66, 0.6)]),
+        ("exact", "rzz", [G.r2(G.RZZ, 66, 67, 0.3)]),
+        ("exact", "truncate", [G.truncate()]),
+        ("exact", "clifford_h_x4", [G.g1(G.H, q) for q in (10, 40, 70, 100)]),
+        ("exact", "pauli_error_x4", [G.pauli_error(q, (0.01, 0.02, 0.03)) for q in (10, 40, 70, 100)]),
+        ("exact", "amplitude_damping", [G.amplitude_damping(66, 0.05)]),
+        ("exact", "tableau_rzz_layer", rzz_layer),
+        ("lossy", "loss_channel", [G.loss_channel(66, 0.05)]),
+        ("set", "rx_run_layer", [G.r1(G.RX, q, 0.6) for q in range(n)] + [G.truncate()]),
+    ]
+    base, base_mode = None, None
+    for mode, name, ops in cases:  # grouped by mode: one base sum on the device at a time
+        if mode != base_mode:
+            base = None
+            base = grown(LossyPauliSum if mode == "lossy" else PauliSum, mode != "set")
+            base_mode = mode
+        s = base.copy()
+        gl = ops_array(ops)
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        s.profile(True)
+        with torch.cuda.nvtx.range(f"kf:{name}"):
+            n_in = len(s)
+            s.run(gl)
+            torch.cuda.synchronize()
+        fam = {k: {"launches": v["launches"], "ms": v["ms"], "bytes": v["bytes"],
+                   "gb_s": v["bytes"] / 1e6 / max(v["ms"], 1e-9),
+                   "frac": v["bytes"] / 1e6 / max(v["ms"], 1e-9) / peak}
+               for k, v in s.profile_read().items() if v["launches"]}
+        print(json.dumps({"op": name, "mode": mode, "terms_in": n_in, "terms_out": len(s),
+                          "families": fam, "peak_gb_s": peak, "peak_kind": peak_kind}), flush=True)
+        del s
+    base = None
+    s = grown(PauliSum, True)
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
+    s.profile(True)
+    with torch.cuda.nvtx.range("kf:overlap_with_zero"):
+        s.overlap_with_zero()
+    fam = {k: v for k, v in s.profile_read().items() if v["launches"]}
+    print(json.dumps({"op": "overlap_with_zero", "mode": "exact", "terms_in": len(s), "families": fam}), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "layer_bandwidth":
         run_layer_bandwidth(args)
+        return
+    if args.workload == "kernel_families":
+        run_kernel_families(args)
         return
     if args.workload == "learned_kicked_ising":
         if args.impl == "reference":

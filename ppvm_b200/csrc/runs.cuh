@@ -28,7 +28,8 @@ namespace ppvm {
 
 constexpr int kRunMaxK = 10;       // groups up to 2^10 coordinates in shared memory
 constexpr int kRunMaxGates = 256;  // gates per fused run
-constexpr int kRunWarps = 4;       // groups per block tile
+constexpr int kRunWarps = 4;       // warps of a k_run_groups block
+constexpr int kRunTileGroups = 16; // groups per look-back tile of k_run_groups (at most 32)
 constexpr unsigned long long kRunLogScratchBit = 1ull << 63;  // in the op log of a run's first gate
 constexpr int kErrFallback = 4;    // device error: a group exceeds kRunMaxK; rerun per gate
 
@@ -430,10 +431,186 @@ __device__ __forceinline__ void run_commit(Ctrl* ctrl, RunScratch R, int op0, in
   }
 }
 
-// One warp per group: butterfly over the group's coordinates, gates in run order.  Warps
-// are independent: each takes its next group by ticket, so groups of very different sizes do
-// not hold each other up at block barriers.  The group number is also the look-back tile,
-// which places every group's survivors after those of all lower-numbered groups.
+// A group of a fused run as one warp holds it: key, coordinate qubits (ascending), whether
+// its weight passes the cap.  Its coefficients and existence bits live in the warp's
+// shared-memory slots, its coordinate bits in gate order in the warp's order array.
+template <int W>
+struct RunGroup {
+  uint64_t v[W], f0[W];
+  uint16_t pos[kRunMaxK];
+  unsigned k;
+  bool wok;
+};
+
+// Loads group g into the warp's slots: key, coordinates, their gate order, members.
+template <int W>
+__device__ __forceinline__ void group_load(RunGroup<W>& G, unsigned long long g, const RunDesc* rd,
+                                           const RunScratch& R, const uint16_t* s_gidx, uint8_t* ord, double* coef,
+                                           unsigned* ex, bool wcap, unsigned long long maxw) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t start = R.g_start[g], cnt = R.g_cnt[g];  // loaded beside the group key
+  uint64_t M[W];
+  G.k = 0;
+  {
+    const uint64_t* gk = R.gkey + g * 2 * W;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      G.v[w] = gk[w];
+      G.f0[w] = gk[W + w];
+      M[w] = G.v[w] & rd->Q[w];
+    }
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      uint64_t m = M[w];
+      while (m) {
+        const int b = __ffsll((long long)m) - 1;
+        G.pos[G.k++] = (uint16_t)(w * 64 + b);
+        m &= m - 1;
+      }
+    }
+  }
+  {  // coordinate bits sorted by the position of their gate in the run (distinct): lane t
+     // takes bit t, its rank is the number of bits whose gate comes earlier
+    unsigned key = 0xFFFFu;
+    for (unsigned t = 0; t < G.k; ++t)
+      if (t == lane) key = s_gidx[G.pos[t]];
+    unsigned rank = 0;
+    for (unsigned t = 0; t < G.k; ++t) rank += __shfl_sync(kFull, key, t) < key;
+    if (lane < G.k) ord[rank] = (uint8_t)lane;
+  }
+  G.wok = true;
+  if (wcap) {
+    unsigned wt = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) wt += __popcll(G.v[w] | G.f0[w]);
+    G.wok = wt <= maxw;  // M is inside v, so every member has this weight
+  }
+  const unsigned size = 1u << G.k;
+  for (unsigned e = lane; e < (size + 31) / 32; e += 32) ex[e] = 0u;
+  __syncwarp();
+  for (uint32_t m = lane; m < cnt; m += 32) {
+    const unsigned c = R.mcoord[start + m];
+    coef[c] = R.mcoef[start + m];
+    atomicOr(&ex[c >> 5], 1u << (c & 31));
+  }
+  __syncwarp();
+}
+
+// The gates of the run in order over the group's slots; children created per gate go to
+// s_created when it is given.  eps of a member with bit t = b:
+//   RX: eps = b ? -1 : +1   (crates/ppvm-pauli-sum/src/sum/rot1.rs:73)
+//   RZ: eps = b ? +1 : -1   (rot1.rs:124)
+template <int W>
+__device__ __forceinline__ void group_butterfly(const RunGroup<W>& G, uint32_t cls, const uint8_t* ord,
+                                                const uint16_t* s_gidx, const double* s_cs, const double* s_sn,
+                                                double* coef, unsigned* ex, unsigned long long* s_created) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned size = 1u << G.k;
+  const double eps_a = cls == 0 ? 1.0 : -1.0, eps_b = -eps_a;
+  for (unsigned r = 0; r < G.k; ++r) {
+    const unsigned t = ord[r];
+    const unsigned j = s_gidx[G.pos[t]];
+    const unsigned bit = 1u << t;
+    const double cs = s_cs[j], sn = s_sn[j];
+    unsigned made = 0;
+    for (unsigned p = lane; p < size / 2; p += 32) {
+      const unsigned a = ((p >> t) << (t + 1)) | (p & (bit - 1));
+      const unsigned b = a | bit;
+      const bool ea = (ex[a >> 5] >> (a & 31)) & 1u, eb = (ex[b >> 5] >> (b & 31)) & 1u;
+      if (ea && eb) {
+        const double ca = coef[a], cb = coef[b];
+        coef[a] = __dadd_rn(__dmul_rn(ca, cs), __dmul_rn(cb, eps_b * sn));
+        coef[b] = __dadd_rn(__dmul_rn(cb, cs), __dmul_rn(ca, eps_a * sn));
+      } else if (ea) {
+        const double ca = coef[a];
+        coef[a] = __dmul_rn(ca, cs);
+        coef[b] = __dmul_rn(ca, eps_a * sn);
+        atomicOr(&ex[b >> 5], 1u << (b & 31));
+        ++made;
+      } else if (eb) {
+        const double cb = coef[b];
+        coef[b] = __dmul_rn(cb, cs);
+        coef[a] = __dmul_rn(cb, eps_b * sn);
+        atomicOr(&ex[a >> 5], 1u << (a & 31));
+        ++made;
+      }
+    }
+    __syncwarp();
+    if (s_created) {
+#pragma unroll
+      for (int o = 16; o; o >>= 1) made += __shfl_down_sync(kFull, made, o);
+      if (lane == 0 && made) atomicAdd(&s_created[j], (unsigned long long)made);
+    }
+  }
+}
+
+// Survivors of the group (existing slots that pass the run's TRUNCATE), on every lane.
+template <int W>
+__device__ __forceinline__ unsigned group_count(const RunGroup<W>& G, const double* coef, const unsigned* ex,
+                                                int trunc, double thr) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned size = 1u << G.k;
+  unsigned mine = 0;
+  for (unsigned c = lane; c < size; c += 32) {
+    const bool e = (ex[c >> 5] >> (c & 31)) & 1u;
+    bool keep = e;
+    if (trunc && e) keep = G.wok && !(fabs(coef[c]) < thr);
+    mine += keep;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(kFull, mine, o);
+  return __shfl_sync(kFull, mine, 0);
+}
+
+// Writes the group's survivors, in coordinate order, to D from index out on.
+template <int W>
+__device__ __forceinline__ void group_write(const RunGroup<W>& G, Planes D, unsigned long long out, uint32_t cls,
+                                            const double* coef, const unsigned* ex, int trunc, double thr) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned size = 1u << G.k;
+  for (unsigned c0 = 0; c0 < size; c0 += 32) {
+    const unsigned c = c0 + lane;
+    bool keep = false;
+    if (c < size) {
+      keep = (ex[c >> 5] >> (c & 31)) & 1u;
+      if (trunc && keep) keep = G.wok && !(fabs(coef[c]) < thr);
+    }
+    const unsigned bal = __ballot_sync(kFull, keep);
+    if (keep) {
+      const unsigned long long r = out + __popc(bal & ((1u << lane) - 1u));
+      if (r < D.cap) {
+        uint64_t f[W], x[W], z[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) f[w] = G.f0[w];
+        for (unsigned t = 0; t < G.k; ++t)
+          if ((c >> t) & 1u) {
+            const unsigned q = G.pos[t];
+#pragma unroll
+            for (int w = 0; w < W; ++w)
+              if (w == (int)(q >> 6)) f[w] |= 1ull << (q & 63);
+          }
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          x[w] = cls == 0 ? f[w] : G.v[w];
+          z[w] = cls == 0 ? G.v[w] : f[w];
+        }
+        store_key<W>(D, r, x, z);
+        D.c[r] = coef[c];
+      }
+    }
+    out += __popc(bal);
+  }
+}
+
+// Groups of a run, kRunTileGroups to a block tile taken by ticket; warp w of the block takes
+// the tile's groups w, w + kRunWarps, ...  Look-back mode: the warps run every group's
+// butterfly and count its survivors, a block scan orders the counts, one decoupled look-back
+// per tile places the tile after all lower tiles, and the warps then write: each warp's last
+// group straight from its slots, the others after running their butterflies again (the same
+// arithmetic in the same order, so the same coefficients).  One look-back per tile instead of
+// one per group.  Scratch mode (many groups): each group's survivors go to the scratch planes
+// S wherever a counter puts them, at once; k_run_place then moves every group's block to its
+// place in O.
 template <int W>
 __global__ void __launch_bounds__(kRunWarps * 32)
 k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, int trunc, double thr,
@@ -441,12 +618,16 @@ k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
              unsigned long long scratch_min) {
   pdl_wait();
   constexpr int SZ = 1 << kRunMaxK;
+  constexpr int GT = kRunTileGroups;
   __shared__ double s_coef[kRunWarps][SZ];
   __shared__ unsigned s_ex[kRunWarps][SZ / 32];
   __shared__ unsigned long long s_created[kRunMaxGates];
   __shared__ double s_cs[kRunMaxGates], s_sn[kRunMaxGates];
   __shared__ uint16_t s_gidx[64 * W];               // qubit -> its gate's index in the run
   __shared__ uint8_t s_ord[kRunWarps][kRunMaxK];    // a group's coordinate bits in gate order
+  __shared__ unsigned s_cnt[GT], s_off[GT + 1];
+  __shared__ unsigned s_tile;
+  __shared__ unsigned long long s_slot;
   __shared__ int s_err;
   if (threadIdx.x == 0) s_err = ld_volatile_int(&ctrl->err);
   const uint32_t L = rd->L;
@@ -466,161 +647,62 @@ k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   const bool wcap = maxw != ~0ull;
   double* coef = s_coef[warp];
   unsigned* ex = s_ex[warp];
+  uint8_t* ord = s_ord[warp];
+  const unsigned long long ntiles = (ngroups + GT - 1) / GT;
   for (;;) {
-    unsigned long long g = 0;
-    if (lane == 0) g = atomicAdd(&ctrl->tickets[2], 1ull);
-    g = __shfl_sync(kFull, g, 0);
-    if (g >= ngroups) break;
-    uint64_t v[W], f0[W], M[W];
-    unsigned k = 0;
-    uint16_t pos[kRunMaxK];  // qubit of coordinate bit t (ascending)
-    bool wok = true;
-    const uint32_t start = R.g_start[g], cnt = R.g_cnt[g];  // loaded beside the group key
-    {
-      const uint64_t* gk = R.gkey + g * 2 * W;
-#pragma unroll
-      for (int w = 0; w < W; ++w) {
-        v[w] = gk[w];
-        f0[w] = gk[W + w];
-        M[w] = v[w] & rd->Q[w];
-      }
-#pragma unroll
-      for (int w = 0; w < W; ++w) {
-        uint64_t m = M[w];
-        while (m) {
-          const int b = __ffsll((long long)m) - 1;
-          pos[k++] = (uint16_t)(w * 64 + b);
-          m &= m - 1;
+    const unsigned tile = next_tile(&ctrl->tickets[2], &s_tile);
+    if (tile >= ntiles) break;
+    const unsigned long long g0 = (unsigned long long)tile * GT;
+    const unsigned ng = (unsigned)min((unsigned long long)GT, ngroups - g0);
+    RunGroup<W> G;
+    unsigned last = GT;  // this warp's last group of the tile (its slots stay loaded)
+    for (unsigned j = warp; j < ng; j += kRunWarps) {
+      group_load<W>(G, g0 + j, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
+      group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, s_created);
+      const unsigned mine = group_count<W>(G, coef, ex, trunc, thr);
+      if (scratch) {
+        unsigned long long b = 0;
+        if (lane == 0) {
+          b = atomicAdd(&ctrl->scr_top, (unsigned long long)mine);
+          R.g_rep[g0 + j] = (uint32_t)(b < 0xFFFFFFFFull ? b : 0xFFFFFFFFull);  // scratch offset (< 2^32)
+          R.g_fill[g0 + j] = mine;                                                // survivors
         }
+        group_write<W>(G, S, __shfl_sync(kFull, b, 0), cls, coef, ex, trunc, thr);
+      } else if (lane == 0) {
+        s_cnt[j] = mine;
       }
+      last = j;
+      __syncwarp();  // the slots and the order array are rewritten by the warp's next group
     }
-    const unsigned size = 1u << k;
-    {  // coordinate bits sorted by the position of their gate in the run (distinct): lane t
-       // takes bit t, its rank is the number of bits whose gate comes earlier
-      unsigned key = 0xFFFFu;
-      for (unsigned t = 0; t < k; ++t)
-        if (t == lane) key = s_gidx[pos[t]];
-      unsigned rank = 0;
-      for (unsigned t = 0; t < k; ++t) rank += __shfl_sync(kFull, key, t) < key;
-      if (lane < k) s_ord[warp][rank] = (uint8_t)lane;
-    }
-    if (wcap) {
-      unsigned wt = 0;
+    if (scratch) continue;  // next_tile's barriers separate the tiles
+    __syncthreads();
+    if (warp == 0) {  // exclusive scan of the tile's counts (GT <= 32)
+      const unsigned c = lane < ng ? s_cnt[lane] : 0u;
+      unsigned v = c;
 #pragma unroll
-      for (int w = 0; w < W; ++w) wt += __popcll(v[w] | f0[w]);
-      wok = wt <= maxw;  // M is inside v, so every member has this weight
-    }
-    for (unsigned e = lane; e < (size + 31) / 32; e += 32) ex[e] = 0u;
-    __syncwarp();
-    for (uint32_t m = lane; m < cnt; m += 32) {
-      const unsigned c = R.mcoord[start + m];
-      coef[c] = R.mcoef[start + m];
-      atomicOr(&ex[c >> 5], 1u << (c & 31));
-    }
-    __syncwarp();
-    // gates of the run in order; eps of a member with bit t = b:
-    //   RX: eps = b ? -1 : +1   (crates/ppvm-pauli-sum/src/sum/rot1.rs:73)
-    //   RZ: eps = b ? +1 : -1   (rot1.rs:124)
-    const double eps_a = cls == 0 ? 1.0 : -1.0, eps_b = -eps_a;
-    for (unsigned r = 0; r < k; ++r) {
-      const unsigned t = s_ord[warp][r];
-      const unsigned j = s_gidx[pos[t]];
-      const unsigned bit = 1u << t;
-      const double cs = s_cs[j], sn = s_sn[j];
-      unsigned made = 0;
-      for (unsigned p = lane; p < size / 2; p += 32) {
-        const unsigned a = ((p >> t) << (t + 1)) | (p & (bit - 1));
-        const unsigned b = a | bit;
-        const bool ea = (ex[a >> 5] >> (a & 31)) & 1u, eb = (ex[b >> 5] >> (b & 31)) & 1u;
-        if (ea && eb) {
-          const double ca = coef[a], cb = coef[b];
-          coef[a] = __dadd_rn(__dmul_rn(ca, cs), __dmul_rn(cb, eps_b * sn));
-          coef[b] = __dadd_rn(__dmul_rn(cb, cs), __dmul_rn(ca, eps_a * sn));
-        } else if (ea) {
-          const double ca = coef[a];
-          coef[a] = __dmul_rn(ca, cs);
-          coef[b] = __dmul_rn(ca, eps_a * sn);
-          atomicOr(&ex[b >> 5], 1u << (b & 31));
-          ++made;
-        } else if (eb) {
-          const double cb = coef[b];
-          coef[b] = __dmul_rn(cb, cs);
-          coef[a] = __dmul_rn(cb, eps_b * sn);
-          atomicOr(&ex[a >> 5], 1u << (a & 31));
-          ++made;
-        }
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(kFull, v, o);
+        if (lane >= (unsigned)o) v += t;
       }
+      if (lane < GT) s_off[lane] = v - c;
+      if (lane == 31) s_off[GT] = v;
+    }
+    __syncthreads();
+    const unsigned long long total = s_off[GT];
+    const unsigned long long excl = lookback(ts, tile, total, epoch, ctrl, op, &s_slot);
+    const unsigned long long out0 = ubase + excl;
+    if (last < GT) group_write<W>(G, O, out0 + s_off[last], cls, coef, ex, trunc, thr);
+    for (unsigned j = warp; j < last; j += kRunWarps) {
       __syncwarp();
-#pragma unroll
-      for (int o = 16; o; o >>= 1) made += __shfl_down_sync(kFull, made, o);
-      if (lane == 0 && made) atomicAdd(&s_created[j], (unsigned long long)made);
+      group_load<W>(G, g0 + j, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
+      group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, nullptr);
+      group_write<W>(G, O, out0 + s_off[j], cls, coef, ex, trunc, thr);
     }
-    // survivors, in coordinate order
-    unsigned mine = 0;
-    for (unsigned c = lane; c < size; c += 32) {
-      const bool e = (ex[c >> 5] >> (c & 31)) & 1u;
-      bool keep = e;
-      if (trunc && e) keep = wok && !(fabs(coef[c]) < thr);
-      mine += keep;
+    __syncwarp();
+    if (tile == ntiles - 1 && threadIdx.x == 0) {
+      ctrl->cap_needed = out0 + total;
+      if (out0 + total > O.cap) set_err(ctrl, kErrCapacity, op);
     }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(kFull, mine, o);
-    mine = __shfl_sync(kFull, mine, 0);
-    // The group's output position.  Look-back mode: after all lower-numbered groups, found by
-    // a warp-level look-back.  Scratch mode (many groups): wherever a counter puts it in the
-    // scratch planes S; k_run_place then moves every group's block to its place in O.
-    unsigned long long excl = 0, out;
-    Planes D = O;
-    if (scratch) {
-      unsigned long long b = 0;
-      if (lane == 0) {
-        b = atomicAdd(&ctrl->scr_top, (unsigned long long)mine);
-        R.g_rep[g] = (uint32_t)(b < 0xFFFFFFFFull ? b : 0xFFFFFFFFull);  // scratch offset (< capacity < 2^32)
-        R.g_fill[g] = mine;                                                      // survivors
-      }
-      out = __shfl_sync(kFull, b, 0);
-      D = S;
-    } else {
-      excl = warp_lookback(ts, g, mine, epoch, ctrl, op);
-      out = ubase + excl;
-    }
-    for (unsigned c0 = 0; c0 < size; c0 += 32) {
-      const unsigned c = c0 + lane;
-      bool keep = false;
-      if (c < size) {
-        keep = (ex[c >> 5] >> (c & 31)) & 1u;
-        if (trunc && keep) keep = wok && !(fabs(coef[c]) < thr);
-      }
-      const unsigned bal = __ballot_sync(kFull, keep);
-      if (keep) {
-        const unsigned long long r = out + __popc(bal & ((1u << lane) - 1u));
-        if (r < D.cap) {
-          uint64_t f[W], x[W], z[W];
-#pragma unroll
-          for (int w = 0; w < W; ++w) f[w] = f0[w];
-          for (unsigned t = 0; t < k; ++t)
-            if ((c >> t) & 1u) {
-              const unsigned q = pos[t];
-#pragma unroll
-              for (int w = 0; w < W; ++w)
-                if (w == (int)(q >> 6)) f[w] |= 1ull << (q & 63);
-            }
-#pragma unroll
-          for (int w = 0; w < W; ++w) {
-            x[w] = cls == 0 ? f[w] : v[w];
-            z[w] = cls == 0 ? v[w] : f[w];
-          }
-          store_key<W>(D, r, x, z);
-          D.c[r] = coef[c];
-        }
-      }
-      out += __popc(bal);
-    }
-    if (!scratch && g == ngroups - 1 && lane == 0) {
-      ctrl->cap_needed = ubase + excl + mine;
-      if (ubase + excl + mine > O.cap) set_err(ctrl, kErrCapacity, op);
-    }
-    __syncwarp();  // coef, ex and s_ord of this warp are rewritten by its next group
   }
   __syncthreads();
   for (unsigned j = threadIdx.x; j < L; j += blockDim.x)
