@@ -310,6 +310,19 @@ unsigned long long run_scratch_min_groups() {
   return v;
 }
 
+// k_run_groups' tiled mode (one look-back per tile of groups): 0 chooses per run (tiled when
+// most groups hold a single member), 1 always, 2 never.  PPVM_RUN_TILED=always|never
+// overrides the choice; the tests run the fused-run cases both ways.
+unsigned run_tile_mode() {
+  static const unsigned v = [] {
+    const char* e = std::getenv("PPVM_RUN_TILED");
+    if (e && std::strcmp(e, "always") == 0) return 1u;
+    if (e && std::strcmp(e, "never") == 0) return 2u;
+    return 0u;
+  }();
+  return v;
+}
+
 // Polls a look-back waits for its predecessors before it gives up with PPVM_ETIMEOUT.  0 (the
 // default) leaves the device's bound of 2^22 polls; PPVM_SPIN_LIMIT overrides it, read once
 // per process (the timeout test sets a few polls, so that a multi-tile look-back gives up).
@@ -1020,7 +1033,7 @@ struct K {
       }
       launch(k_run_groups<W>, grid_for(nub, kRunWarps, std::min(resident, 8)), kRunWarps * 32, 0, s->stream,
           O, S, s->d_ctrl, d_rd, s->R, trunc, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0,
-          trunc_op, s->d_log, scratch_min);  // its last block publishes the counts and the op log
+          trunc_op, s->d_log, scratch_min, run_tile_mode());  // its last block publishes the counts and the op log
     }
     if (allow) {
       ProfScope ps(s, F_RUN_PLACE, op0, L);

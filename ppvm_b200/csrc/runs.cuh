@@ -30,6 +30,7 @@ constexpr int kRunMaxK = 10;       // groups up to 2^10 coordinates in shared me
 constexpr int kRunMaxGates = 256;  // gates per fused run
 constexpr int kRunWarps = 4;       // warps of a k_run_groups block
 constexpr int kRunTileGroups = 16; // groups per look-back tile of k_run_groups (at most 32)
+constexpr unsigned long long kRunTileMinGroups = 8192;  // fewer groups: one look-back per group
 constexpr unsigned long long kRunLogScratchBit = 1ull << 63;  // in the op log of a run's first gate
 constexpr int kErrFallback = 4;    // device error: a group exceeds kRunMaxK; rerun per gate
 
@@ -602,20 +603,28 @@ __device__ __forceinline__ void group_write(const RunGroup<W>& G, Planes D, unsi
   }
 }
 
-// Groups of a run, kRunTileGroups to a block tile taken by ticket; warp w of the block takes
-// the tile's groups w, w + kRunWarps, ...  Look-back mode: the warps run every group's
-// butterfly and count its survivors, a block scan orders the counts, one decoupled look-back
-// per tile places the tile after all lower tiles, and the warps then write: each warp's last
-// group straight from its slots, the others after running their butterflies again (the same
-// arithmetic in the same order, so the same coefficients).  One look-back per tile instead of
-// one per group.  Scratch mode (many groups): each group's survivors go to the scratch planes
-// S wherever a counter puts them, at once; k_run_place then moves every group's block to its
-// place in O.
+// The groups of a run, in one of three modes chosen per launch (the same in every block):
+// - one group per warp, taken by ticket (groups of several members): the warp runs the
+//   butterfly, counts the survivors, finds the group's output offset by a warp look-back over
+//   the lower-numbered groups, and writes;
+// - tiles of kRunTileGroups groups per block (at least kRunTileMinGroups groups of fewer
+//   than 1.5 members on average, or tile_mode 1): warp w takes the tile's groups w,
+//   w + kRunWarps, ...; the warps run every butterfly and count, a block scan orders the
+//   counts, one decoupled look-back places the tile after all lower tiles, and the warps then
+//   write, each warp's last group straight from its slots and the others after running their
+//   butterflies again (the same arithmetic in the same order, so the same coefficients).  One
+//   look-back per tile instead of per group; the second butterfly costs less than the
+//   look-backs it saves only when the butterflies are short;
+// - scratch mode (many groups): one group per warp, its survivors written at once to the
+//   scratch planes S wherever a counter puts them; k_run_place then moves every group's
+//   block to its place in O.
+// Every mode writes the same terms in the same order: groups by number, members by
+// coordinate.
 template <int W>
 __global__ void __launch_bounds__(kRunWarps * 32)
 k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, int trunc, double thr,
              unsigned long long maxw, unsigned long long* ts, unsigned epoch, int op, int trunc_op, OpLog* log,
-             unsigned long long scratch_min) {
+             unsigned long long scratch_min, unsigned tile_mode) {
   pdl_wait();
   constexpr int SZ = 1 << kRunMaxK;
   constexpr int GT = kRunTileGroups;
@@ -648,60 +657,89 @@ k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   double* coef = s_coef[warp];
   unsigned* ex = s_ex[warp];
   uint8_t* ord = s_ord[warp];
-  const unsigned long long ntiles = (ngroups + GT - 1) / GT;
-  for (;;) {
-    const unsigned tile = next_tile(&ctrl->tickets[2], &s_tile);
-    if (tile >= ntiles) break;
-    const unsigned long long g0 = (unsigned long long)tile * GT;
-    const unsigned ng = (unsigned)min((unsigned long long)GT, ngroups - g0);
-    RunGroup<W> G;
-    unsigned last = GT;  // this warp's last group of the tile (its slots stay loaded)
-    for (unsigned j = warp; j < ng; j += kRunWarps) {
-      group_load<W>(G, g0 + j, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
+  // Many mostly single-member groups (runs over sums whose terms rarely share a group; their
+  // butterflies are short) go in block tiles: there the per-group look-backs cost more than
+  // running the butterflies twice.  Groups of several members (long butterflies), and runs
+  // of few groups (which tiles would spread over too few warps), go one per warp.
+  // tile_mode 1 or 2 forces either.  The choice is the same in every block.
+  const unsigned long long members = ld_volatile(&ctrl->n_side);
+  const bool tiled = !scratch && (tile_mode == 1 || (tile_mode == 0 && ngroups >= kRunTileMinGroups &&
+                                                     2 * members < 3 * ngroups));
+  if (!tiled) {
+    for (;;) {
+      unsigned long long g = 0;
+      if (lane == 0) g = atomicAdd(&ctrl->tickets[2], 1ull);
+      g = __shfl_sync(kFull, g, 0);
+      if (g >= ngroups) break;
+      RunGroup<W> G;
+      group_load<W>(G, g, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
       group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, s_created);
       const unsigned mine = group_count<W>(G, coef, ex, trunc, thr);
       if (scratch) {
         unsigned long long b = 0;
         if (lane == 0) {
           b = atomicAdd(&ctrl->scr_top, (unsigned long long)mine);
-          R.g_rep[g0 + j] = (uint32_t)(b < 0xFFFFFFFFull ? b : 0xFFFFFFFFull);  // scratch offset (< 2^32)
-          R.g_fill[g0 + j] = mine;                                                // survivors
+          R.g_rep[g] = (uint32_t)(b < 0xFFFFFFFFull ? b : 0xFFFFFFFFull);  // scratch offset (< capacity < 2^32)
+          R.g_fill[g] = mine;                                                // survivors
         }
         group_write<W>(G, S, __shfl_sync(kFull, b, 0), cls, coef, ex, trunc, thr);
-      } else if (lane == 0) {
-        s_cnt[j] = mine;
+      } else {
+        const unsigned long long excl = warp_lookback(ts, g, mine, epoch, ctrl, op);
+        group_write<W>(G, O, ubase + excl, cls, coef, ex, trunc, thr);
+        if (g == ngroups - 1 && lane == 0) {
+          ctrl->cap_needed = ubase + excl + mine;
+          if (ubase + excl + mine > O.cap) set_err(ctrl, kErrCapacity, op);
+        }
       }
-      last = j;
       __syncwarp();  // the slots and the order array are rewritten by the warp's next group
     }
-    if (scratch) continue;  // next_tile's barriers separate the tiles
-    __syncthreads();
-    if (warp == 0) {  // exclusive scan of the tile's counts (GT <= 32)
-      const unsigned c = lane < ng ? s_cnt[lane] : 0u;
-      unsigned v = c;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned t = __shfl_up_sync(kFull, v, o);
-        if (lane >= (unsigned)o) v += t;
+  } else {
+    const unsigned long long ntiles = (ngroups + GT - 1) / GT;
+    for (;;) {
+      const unsigned tile = next_tile(&ctrl->tickets[2], &s_tile);
+      if (tile >= ntiles) break;
+      const unsigned long long g0 = (unsigned long long)tile * GT;
+      const unsigned ng = (unsigned)min((unsigned long long)GT, ngroups - g0);
+      RunGroup<W> G;
+      unsigned last = GT;  // this warp's last group of the tile (its slots stay loaded)
+      for (unsigned j = warp; j < ng; j += kRunWarps) {
+        group_load<W>(G, g0 + j, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
+        group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, s_created);
+        const unsigned mine = group_count<W>(G, coef, ex, trunc, thr);
+        if (lane == 0) s_cnt[j] = mine;
+        last = j;
+        __syncwarp();  // the slots and the order array are rewritten by the warp's next group
       }
-      if (lane < GT) s_off[lane] = v - c;
-      if (lane == 31) s_off[GT] = v;
-    }
-    __syncthreads();
-    const unsigned long long total = s_off[GT];
-    const unsigned long long excl = lookback(ts, tile, total, epoch, ctrl, op, &s_slot);
-    const unsigned long long out0 = ubase + excl;
-    if (last < GT) group_write<W>(G, O, out0 + s_off[last], cls, coef, ex, trunc, thr);
-    for (unsigned j = warp; j < last; j += kRunWarps) {
+      __syncthreads();
+      if (warp == 0) {  // exclusive scan of the tile's counts (GT <= 32)
+        const unsigned c = lane < ng ? s_cnt[lane] : 0u;
+        unsigned v = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned t = __shfl_up_sync(kFull, v, o);
+          if (lane >= (unsigned)o) v += t;
+        }
+        if (lane < GT) s_off[lane] = v - c;
+        if (lane == 31) s_off[GT] = v;
+      }
+      __syncthreads();
+      const unsigned long long total = s_off[GT];
+      const unsigned long long excl = lookback(ts, tile, total, epoch, ctrl, op, &s_slot);
+      const unsigned long long out0 = ubase + excl;
+      if (last < GT) {  // a warp without a group in a short last tile writes nothing
+        group_write<W>(G, O, out0 + s_off[last], cls, coef, ex, trunc, thr);
+        for (unsigned j = warp; j < last; j += kRunWarps) {
+          __syncwarp();
+          group_load<W>(G, g0 + j, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
+          group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, nullptr);
+          group_write<W>(G, O, out0 + s_off[j], cls, coef, ex, trunc, thr);
+        }
+      }
       __syncwarp();
-      group_load<W>(G, g0 + j, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
-      group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, nullptr);
-      group_write<W>(G, O, out0 + s_off[j], cls, coef, ex, trunc, thr);
-    }
-    __syncwarp();
-    if (tile == ntiles - 1 && threadIdx.x == 0) {
-      ctrl->cap_needed = out0 + total;
-      if (out0 + total > O.cap) set_err(ctrl, kErrCapacity, op);
+      if (tile == ntiles - 1 && threadIdx.x == 0) {
+        ctrl->cap_needed = out0 + total;
+        if (out0 + total > O.cap) set_err(ctrl, kErrCapacity, op);
+      }
     }
   }
   __syncthreads();
