@@ -853,7 +853,10 @@ def run_kernel_families(args):
         ("exact", "tableau_rzz_layer", rzz_layer),
         ("lossy", "loss_channel", [G.loss_channel(66, 0.05)]),
         ("set", "rx_run_layer", [G.r1(G.RX, q, 0.6) for q in range(n)] + [G.truncate()]),
+        ("exact", "overlap_with_zero", None),
+        ("exact", "truncate_budget_half", None),
     ]
+    cases.sort(key=lambda c: ("exact", "lossy", "set").index(c[0]))
     base, base_mode = None, None
     for mode, name, ops in cases:  # grouped by mode: one base sum on the device at a time
         if mode != base_mode:
@@ -861,30 +864,31 @@ def run_kernel_families(args):
             base = grown(LossyPauliSum if mode == "lossy" else PauliSum, mode != "set")
             base_mode = mode
         s = base.copy()
-        gl = ops_array(ops)
+        gl = ops_array(ops) if ops is not None else None
         flush.fill_(1.0)
         torch.cuda.synchronize()
         s.profile(True)
+        n_in = len(s)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
         with torch.cuda.nvtx.range(f"kf:{name}"):
-            n_in = len(s)
-            s.run(gl)
+            t0.record()
+            if name == "overlap_with_zero":
+                s.overlap_with_zero()
+            elif name == "truncate_budget_half":
+                s.truncate_budget(n_in // 2)
+            else:
+                s.run(gl)
+            t1.record()
             torch.cuda.synchronize()
         fam = {k: {"launches": v["launches"], "ms": v["ms"], "bytes": v["bytes"],
                    "gb_s": v["bytes"] / 1e6 / max(v["ms"], 1e-9),
                    "frac": v["bytes"] / 1e6 / max(v["ms"], 1e-9) / peak}
                for k, v in s.profile_read().items() if v["launches"]}
         print(json.dumps({"op": name, "mode": mode, "terms_in": n_in, "terms_out": len(s),
-                          "families": fam, "peak_gb_s": peak, "peak_kind": peak_kind}), flush=True)
+                          "call_ms": t0.elapsed_time(t1), "families": fam, "peak_gb_s": peak,
+                          "peak_kind": peak_kind}), flush=True)
         del s
-    base = None
-    s = grown(PauliSum, True)
-    flush.fill_(1.0)
-    torch.cuda.synchronize()
-    s.profile(True)
-    with torch.cuda.nvtx.range("kf:overlap_with_zero"):
-        s.overlap_with_zero()
-    fam = {k: v for k, v in s.profile_read().items() if v["launches"]}
-    print(json.dumps({"op": "overlap_with_zero", "mode": "exact", "terms_in": len(s), "families": fam}), flush=True)
 
 
 def main():

@@ -89,6 +89,7 @@ struct ProfLaunch {
   int op;
   int nops;  // ops covered (Clifford runs)
   int aux;   // fused TRUNCATE op of a tableau pass, else -1
+  uint64_t bytes;  // algorithmic bytes of a launch outside the op list (op < 0), else unused
   cudaEvent_t a, b;
 };
 
@@ -566,6 +567,7 @@ struct ProfScope {
     L.op = op;
     L.nops = nops;
     L.aux = aux;
+    L.bytes = 0;
     L.a = take();
     L.b = take();
     cudaEventRecord(L.a, s->stream);
@@ -610,6 +612,7 @@ uint64_t launch_bytes(const ppvm_sum* s, const ProfLaunch& L, const std::vector<
       const OpLog& last = s->h_log[L.op + std::max(L.nops, 1) - 1];
       return (g.n_s & ~kRunLogScratchBit) * B + (L.nops > 1 ? last.n_s : 0) * B;
     }
+    case F_LOSS: return g.n_in * B + g.n_out * B;  // every term read once, every output written once
     case F_RUN_PLACE: {  // scratch mode: group outputs read from the scratch, written to their place
       if (!(g.n_s & kRunLogScratchBit)) return 0;  // look-back mode: the kernel returned at once
       const OpLog& last = s->h_log[L.op + std::max(L.nops, 1) - 1];
@@ -626,6 +629,7 @@ void prof_collect(ppvm_sum* s, const std::vector<int>& test_words) {
     s->prof_ms[L.family] += ms;
     s->prof_launches[L.family] += 1;
     if (L.op >= 0 && (size_t)L.op < s->log_cap) s->prof_bytes[L.family] += launch_bytes(s, L, test_words);
+    else if (L.op < 0) s->prof_bytes[L.family] += L.bytes;
     s->event_pool.push_back(L.a);
     s->event_pool.push_back(L.b);
   }
@@ -1107,7 +1111,9 @@ struct K {
   }
 
   static void owz(ppvm_sum* s, int nblocks) {
-    s->launch_count += 2;
+    ProfScope ps(s, F_READ, -1, 1);
+    ps.L.bytes = s->n_host * (8ull * W + 8);  // every term's X words and coefficient
+    s->launch_count += 1;                     // k_sum_partials (ProfScope counts k_owz)
     k_owz<W><<<nblocks, kRedBlock, 0, s->stream>>>(s->planes_view(), s->d_ctrl, s->d_partials);
     k_sum_partials<<<1, kRedBlock, 0, s->stream>>>(s->d_partials, nblocks, s->d_ctrl);
   }
@@ -1447,6 +1453,7 @@ ppvm_status do_reduce_owz(ppvm_sum* s, double* out) {
   DISPATCH_W(s->W, owz(s, nb));
   CUDA_TRY(cudaGetLastError());
   PPVM_TRY(sync_state(s, 0));
+  if (s->prof) prof_collect(s, {});
   *out = s->h_ctrl->sum;
   return PPVM_OK;
 }
