@@ -938,11 +938,18 @@ struct K {
       ProfScope ps(s, F_LOSS, op, 1);
       launch(k_loss_index<W>, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, s->table, tsize - 1, tep,
              op, s->d_log);
-      launch(k_loss_count<W>, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, lo, s->table, tsize - 1,
-             tep);
       const unsigned e1 = s->next_tile_epoch(), e2 = s->next_tile_epoch();
-      launch(k_loss_emit<W, 256>, grid_for(nub, 256, 8), 256, 0, s->stream, P, O, s->d_ctrl, lo, s->table,
-             tsize - 1, tep, s->tstate, s->tstate2, e1, e2, op, s->d_log);
+      auto count_emit = [&](auto count_k, auto emit_k) {
+        launch(count_k, grid_for(nub, 256, 8), 256, 0, s->stream, P, s->d_ctrl, lo, s->table, tsize - 1, tep);
+        launch(emit_k, grid_for(nub, 256, 8), 256, 0, s->stream, P, O, s->d_ctrl, lo, s->table, tsize - 1, tep,
+               s->tstate, s->tstate2, e1, e2, op, s->d_log);
+      };
+      if (lo.mode == kLossChannel)
+        count_emit(k_loss_count<W, kLossChannel>, k_loss_emit<W, 256, kLossChannel>);
+      else if (lo.mode == kResetLoss)
+        count_emit(k_loss_count<W, kResetLoss>, k_loss_emit<W, 256, kResetLoss>);
+      else
+        count_emit(k_loss_count<W, kCorrelatedLoss>, k_loss_emit<W, 256, kCorrelatedLoss>);
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op);

@@ -266,11 +266,15 @@ k_loss_index(Planes P, Ctrl* ctrl, unsigned long long* table, unsigned long long
     index_insert<W>(P, i, table, mask, tepoch, ctrl);
 }
 
-template <int W>
+// k_loss_count and k_loss_emit are compiled once per channel (M = op.mode): with the mode a
+// constant, each keeps only its channel's children and parents, and far fewer registers.
+template <int W, int M>
 __global__ void __launch_bounds__(256)
-k_loss_count(Planes P, Ctrl* ctrl, LossOp op, const unsigned long long* table, unsigned long long mask,
+k_loss_count(Planes P, Ctrl* ctrl, LossOp op_in, const unsigned long long* table, unsigned long long mask,
              unsigned tepoch) {
   pdl_wait();
+  LossOp op = op_in;
+  op.mode = M;
   __shared__ unsigned long long s_new, s_aux;
   if (ld_volatile_int(&ctrl->err)) return;
   if (threadIdx.x == 0) s_new = s_aux = 0;
@@ -281,9 +285,18 @@ k_loss_count(Planes P, Ctrl* ctrl, LossOp op, const unsigned long long* table, u
        i += (unsigned long long)gridDim.x * blockDim.x) {
     uint64_t x[W], z[W];
     load_key<W>(P, i, x, z);
-    bool first[3], isnew[3];
-    na += loss_children<W>(op, P, i, x, z, table, mask, tepoch, first, isnew);
-    nn += (unsigned)isnew[0] + (unsigned)isnew[1] + (unsigned)isnew[2];
+    if constexpr (M == kLossChannel) {
+      // a lost qubit's term is the only parent of its child (the qubit as I): the child is new
+      // when that key is absent
+      if (loss_code<W>(x, z, op.lw, op.qa) == 4) {
+        loss_set<W>(x, z, op.lw, op.qa, 0);
+        nn += index_find<W>(P, x, z, table, mask, tepoch) < 0;
+      }
+    } else {
+      bool first[3], isnew[3];
+      na += loss_children<W>(op, P, i, x, z, table, mask, tepoch, first, isnew);
+      nn += (unsigned)isnew[0] + (unsigned)isnew[1] + (unsigned)isnew[2];
+    }
   }
   if (nn) atomicAdd(&s_new, nn);
   if (na) atomicAdd(&s_aux, na);
@@ -318,12 +331,14 @@ __device__ __forceinline__ unsigned block_excl(unsigned v, unsigned* s_w, unsign
   return base + inc - v;
 }
 
-template <int W, int BLOCK>
+template <int W, int BLOCK, int M>
 __global__ void __launch_bounds__(BLOCK)
-k_loss_emit(Planes P, Planes O, Ctrl* ctrl, LossOp op, const unsigned long long* table, unsigned long long mask,
+k_loss_emit(Planes P, Planes O, Ctrl* ctrl, LossOp op_in, const unsigned long long* table, unsigned long long mask,
             unsigned tepoch, unsigned long long* ts, unsigned long long* ts2, unsigned epoch, unsigned epoch2,
             int opi, OpLog* log) {
   pdl_wait();
+  LossOp op = op_in;
+  op.mode = M;
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
   __shared__ unsigned s_w[BLOCK / 32];
@@ -341,6 +356,54 @@ k_loss_emit(Planes P, Planes O, Ctrl* ctrl, LossOp op, const unsigned long long*
   // consume keeps the order of the larger map: the child keys' when they outnumber the terms
   const bool aux_first = op.mode == kCorrelatedLoss && n_aux > N;
   const unsigned long long ntiles = (N + BLOCK - 1) / BLOCK;
+  if constexpr (M == kLossChannel) {
+    // per term one index lookup: a term with L on qa keeps v and, when the key with I there is
+    // absent, makes it as a new key with v * p (appended in parent order); a term with I on
+    // qa takes v * (1 - p) plus p times the coefficient of the key with L there, if present;
+    // X, Y, Z take v * (1 - p)
+    for (;;) {
+      const unsigned tile = next_tile(&ctrl->tickets[0], &s_tile);
+      if (tile >= ntiles) break;
+      const unsigned long long i = (unsigned long long)tile * BLOCK + threadIdx.x;
+      uint64_t x[W], z[W];
+      bool isnew = false;
+      double v = 0.0, own = 0.0;
+      if (i < N) {
+        load_key<W>(P, i, x, z);
+        v = P.c[i];
+        const int ca = loss_code<W>(x, z, op.lw, op.qa);
+        if (ca == 4 || ca == 0) {
+          uint64_t kx[W], kz[W];
+#pragma unroll
+          for (int w = 0; w < W; ++w) kx[w] = x[w], kz[w] = z[w];
+          loss_set<W>(kx, kz, op.lw, op.qa, ca == 4 ? 0 : 4);
+          const long long j = index_find<W>(P, kx, kz, table, mask, tepoch);
+          if (ca == 4) {
+            own = v;
+            isnew = j < 0;
+          } else {
+            own = __dmul_rn(v, op.keep1);
+            if (j >= 0) own = __dadd_rn(own, __dmul_rn(P.c[j], op.p0));
+          }
+        } else {
+          own = __dmul_rn(v, op.keep1);
+        }
+      }
+      unsigned t1;
+      const unsigned e1 = block_excl<BLOCK>(isnew ? 1u : 0u, s_w, t1);
+      const unsigned long long x1 = lookback(ts, tile, t1, epoch, ctrl, opi, &s_slot);
+      if (i < N) {
+        store_key<W>(O, i, x, z);
+        O.c[i] = own;
+        if (isnew) {
+          const unsigned long long r = N + x1 + e1;
+          loss_set<W>(x, z, op.lw, op.qa, 0);
+          store_key<W>(O, r, x, z);
+          O.c[r] = __dmul_rn(v, op.p0);
+        }
+      }
+    }
+  } else
   for (;;) {
     const unsigned tile = next_tile(&ctrl->tickets[0], &s_tile);
     if (tile >= ntiles) break;
