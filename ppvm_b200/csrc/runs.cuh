@@ -106,6 +106,7 @@ k_run_classify(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, 
     uint64_t kx[ITEMS][W], kz[ITEMS][W];
     double kc[ITEMS];
     unsigned bal[ITEMS];
+    unsigned fb = 0;  // fallback: the largest gate cut among this thread's wide terms
 #pragma unroll
     for (int it = 0; it < ITEMS; ++it) {
       const unsigned long long i = base + (unsigned long long)it * BLOCK + threadIdx.x;
@@ -151,8 +152,7 @@ k_run_classify(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, 
               hi[r] = gi;
             }
           }
-          atomicMax(&ctrl->fb_cut, (unsigned long long)hi[kRunMaxK] + 1ull);
-          set_err(ctrl, kErrFallback, op);
+          fb = max(fb, hi[kRunMaxK] + 1u);  // reported once per warp below
           R.gslot[i] = kNone;
         } else {
           const uint64_t h = hash_key<W>(v, f);
@@ -188,6 +188,13 @@ k_run_classify(Planes P, Planes O, Ctrl* ctrl, const RunDesc* rd, RunScratch R, 
         }
       }
       bal[it] = __ballot_sync(kFull, keep);
+    }
+    // terms with more than kRunMaxK coordinates: one report per warp instead of one atomic on
+    // the same two words per term (a wide run has millions of such terms)
+    fb = __reduce_max_sync(kFull, fb);
+    if (fb && lane == 0) {
+      if (ld_volatile(&ctrl->fb_cut) < fb) atomicMax(&ctrl->fb_cut, (unsigned long long)fb);
+      if (!ld_volatile_int(&ctrl->err)) set_err(ctrl, kErrFallback, op);
     }
     const unsigned agg = tile_ranks<BLOCK, ITEMS>(bal, s_base);
     const unsigned long long excl = lookback(ts, tile, agg, epoch, ctrl, op, &s_slot);
