@@ -118,6 +118,24 @@ ppvm_status ppvm_sum_add_string(ppvm_sum* sum, const char* word, double c);
 /* preserve_strings of the builder (data.rs:75-77, restore logic data.rs:283-310). */
 ppvm_status ppvm_sum_set_preserve(ppvm_sum* sum, const uint64_t* x, const uint64_t* z, size_t k);
 
+/* ---- one sum spread over several ranks (hash-owner sharding) ---------------------- */
+/* No counterpart in the reference, which keeps a sum in one process.  A sum is split over
+ * n_parts ranks, every key on one rank.  Before a step that merges keys differing in the
+ * bits (mask_x, mask_z) (a rotation: its generator's bits; a fused RX run: the run's qubits
+ * in the X plane; RZ: in the Z plane), every rank calls ppvm_sum_shard_export: its terms go,
+ * as rows of 2W+1 u64 (x[W], z[W], the coefficient's bits) into the DEVICE buffer d_rows
+ * (room for at least len() rows), grouped by owner p = hash(key with the mask bits cleared)
+ * mod n_parts, owners in order and terms in their order within an owner; counts[p] gets each
+ * owner's row count, and the sum is left empty.  The caller exchanges the rows between the
+ * ranks (an all-to-all) and gives each rank the rows it owns with ppvm_sum_shard_append,
+ * which appends them without merging: keys never repeat across ranks.  Every key that the
+ * step can merge then lives on one rank, and the step runs on each rank alone.  n_parts is at
+ * most 32; mask_x and mask_z hold the sum's W words each.  Both calls synchronise the sum's
+ * stream before they return. */
+ppvm_status ppvm_sum_shard_export(ppvm_sum* sum, const uint64_t* mask_x, const uint64_t* mask_z,
+                                  uint32_t n_parts, void* d_rows, size_t rows_cap, uint64_t* counts);
+ppvm_status ppvm_sum_shard_append(ppvm_sum* sum, const void* d_rows, size_t k);
+
 /* len() (data.rs:165-167; interface.rs:389-391). */
 ppvm_status ppvm_len(const ppvm_sum* sum, size_t* out);
 /* terms() (interface.rs:393-395): copies up to cap terms in the sum's iteration order. */

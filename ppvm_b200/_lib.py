@@ -96,6 +96,8 @@ _SIGS = {
     "ppvm_mlp_grad": [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), _SZ,
                       ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
     "ppvm_mlp_predict": [_P, ctypes.POINTER(ctypes.c_float), _SZ, ctypes.POINTER(ctypes.c_float)],
+    "ppvm_sum_shard_export": [_P, _U64P, _U64P, ctypes.c_uint32, _P, _SZ, _U64P],
+    "ppvm_sum_shard_append": [_P, _P, _SZ],
     "ppvm_batch_create": [ctypes.POINTER(_P), _SZ, _U32P, _DP, _U64P, ctypes.c_uint32, _I],
     "ppvm_batch_destroy": [_P],
     "ppvm_batch_set_stream": [_P, _P],

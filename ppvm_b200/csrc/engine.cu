@@ -27,6 +27,7 @@
 #include "budget.cuh"
 #include "loss.cuh"
 #include "noise.cuh"
+#include "shard.cuh"
 
 using namespace ppvm;
 
@@ -1142,6 +1143,22 @@ struct K {
     k_add_terms_seq<W><<<1, 1, 0, s->stream>>>(s->planes_view(), s->d_ctrl, nx, nz, nc, k, s->table,
                                                 mask, ep);
   }
+  // hash-owner sharding: stable partition of the terms by owner into caller rows; append
+  static void shard_export(ppvm_sum* s, const Gen& m, unsigned nparts, unsigned long long ntiles,
+                           unsigned long long* hist, unsigned long long* first, uint64_t* rows) {
+    const Planes P = s->planes_view();
+    const unsigned long long N = s->n_host;
+    k_shard_hist<W><<<(unsigned)ntiles, kShardBlock, 0, s->stream>>>(P, N, m, nparts, hist);
+    k_shard_scan<<<1, 1024, 0, s->stream>>>(hist, ntiles, nparts, first);
+    k_shard_scatter<W><<<(unsigned)ntiles, kShardBlock, 0, s->stream>>>(P, N, m, nparts, hist, rows);
+    k_shard_append<W><<<1, 32, 0, s->stream>>>(P, s->d_ctrl, nullptr, 0ull, 0ull);  // the sum is now empty
+    s->launch_count += 4;
+  }
+  static void shard_append(ppvm_sum* s, const uint64_t* rows, unsigned long long k) {
+    k_shard_append<W><<<(unsigned)grid_for(k, 256, 8), 256, 0, s->stream>>>(s->planes_view(), s->d_ctrl, rows, k,
+                                                                          s->n_host);
+    s->launch_count += 1;
+  }
   static void overlap(ppvm_sum* a, ppvm_sum* b, unsigned long long mask, unsigned ep, int nblocks,
                       unsigned long long* mismatch) {
     k_overlap<W><<<nblocks, kRedBlock, 0, a->stream>>>(a->planes_view(), b->planes_view(), b->d_ctrl,
@@ -1810,6 +1827,66 @@ ppvm_status ppvm_sum_add_terms(ppvm_sum* s, const uint64_t* x, const uint64_t* z
     return fail(PPVM_ECUDA, "device error while adding terms");
   }
   s->n_host = s->h_ctrl->n;
+  s->n_ub = s->n_host;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_sum_shard_export(ppvm_sum* s, const uint64_t* mask_x, const uint64_t* mask_z, uint32_t n_parts,
+                                  void* d_rows, size_t rows_cap, uint64_t* counts) {
+  if (!s || !mask_x || !mask_z || !counts) return fail(PPVM_EINVAL, "null argument");
+  if (n_parts < 1 || n_parts > (uint32_t)kShardMaxParts)
+    return fail(PPVM_EINVAL, "n_parts must be in [1, " + std::to_string(kShardMaxParts) + "]");
+  REQUIRE_USABLE(s);
+  PPVM_TRY(ensure_device(s->device));
+  const unsigned long long N = s->n_host;
+  for (uint32_t p = 0; p < n_parts; ++p) counts[p] = 0;
+  if (N == 0) return PPVM_OK;
+  if (!d_rows) return fail(PPVM_EINVAL, "null row buffer");
+  if (rows_cap < N) return fail(PPVM_EINVAL, "row buffer holds fewer rows than the sum has terms");
+  Gen m;
+  std::memset(&m, 0, sizeof(m));
+  for (int w = 0; w < s->W; ++w) {
+    m.gx[w] = mask_x[w];
+    m.gz[w] = mask_z[w];
+  }
+  const unsigned long long ntiles = (N + kShardBlock - 1) / kShardBlock;
+  unsigned long long* hist = nullptr;
+  CUDA_TRY(pool_malloc((void**)&hist, sizeof(unsigned long long) * (ntiles * n_parts + n_parts + 1)));
+  unsigned long long* first = hist + ntiles * n_parts;
+  DISPATCH_W(s->W, shard_export(s, m, n_parts, ntiles, hist, first, static_cast<uint64_t*>(d_rows)));
+  std::vector<unsigned long long> h_first(n_parts + 1);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h_first.data(), first, sizeof(unsigned long long) * (n_parts + 1), cudaMemcpyDeviceToHost,
+                        s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  pool_free(hist);
+  if (e != cudaSuccess) {
+    s->poisoned = true;
+    return fail(PPVM_ECUDA, std::string("shard export: ") + cudaGetErrorString(e));
+  }
+  for (uint32_t p = 0; p < n_parts; ++p) counts[p] = h_first[p + 1] - h_first[p];
+  s->xfer_d2h += sizeof(unsigned long long) * (n_parts + 1);
+  s->n_host = 0;
+  s->n_ub = 0;
+  return PPVM_OK;
+}
+
+ppvm_status ppvm_sum_shard_append(ppvm_sum* s, const void* d_rows, size_t k) {
+  if (!s) return fail(PPVM_EINVAL, "null sum");
+  REQUIRE_USABLE(s);
+  if (k == 0) return PPVM_OK;
+  if (!d_rows) return fail(PPVM_EINVAL, "null row buffer");
+  PPVM_TRY(ensure_device(s->device));
+  if (s->n_host + k > s->cap) PPVM_TRY(grow(s, std::max<unsigned long long>(2 * s->cap, s->n_host + k + 1024)));
+  DISPATCH_W(s->W, shard_append(s, static_cast<const uint64_t*>(d_rows), k));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);  // the caller may free the rows on return
+  if (e != cudaSuccess) {
+    s->poisoned = true;
+    return fail(PPVM_ECUDA, std::string("shard append: ") + cudaGetErrorString(e));
+  }
+  s->n_host += k;
   s->n_ub = s->n_host;
   return PPVM_OK;
 }
