@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <atomic>
 #include <mutex>
@@ -113,7 +114,7 @@ struct BInst {
 
 constexpr unsigned kBNone = 0xFFFFFFFFu;
 
-unsigned long long region_words(int W, unsigned long long cap, unsigned long long tsize) {
+__host__ __device__ inline unsigned long long region_words(int W, unsigned long long cap, unsigned long long tsize) {
   return (unsigned long long)(2 * W + 3) * cap + tsize;
 }
 
@@ -129,13 +130,12 @@ struct Region {
   unsigned long long cap, tsize;
 };
 
+// The region layout from its first word b (in the pool, or in shared memory).
 template <int W>
-__device__ __forceinline__ Region<W> region_of(uint64_t* pool, const BInst& I) {
+__device__ __forceinline__ Region<W> region_at(uint64_t* b, unsigned long long cap, unsigned long long tsize) {
   Region<W> r;
-  uint64_t* b = pool + I.off;
-  const unsigned long long cap = I.cap;
   r.cap = cap;
-  r.tsize = I.tsize;
+  r.tsize = tsize;
   r.x = b;
   r.z = b + (size_t)W * cap;
   r.c = reinterpret_cast<double*>(b + (size_t)2 * W * cap);
@@ -144,6 +144,10 @@ __device__ __forceinline__ Region<W> region_of(uint64_t* pool, const BInst& I) {
   r.part = r.sidx + cap;
   r.table = reinterpret_cast<unsigned long long*>(b + (size_t)(2 * W + 3) * cap);
   return r;
+}
+template <int W>
+__device__ __forceinline__ Region<W> region_of(uint64_t* pool, const BInst& I) {
+  return region_at<W>(pool + I.off, I.cap, I.tsize);
 }
 
 template <int W>
@@ -297,11 +301,12 @@ __device__ __forceinline__ void block_sum2_u64(unsigned long long& a, unsigned l
 template <int W, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ layer_ends,
-        const double* __restrict__ params, int layer, uint64_t* pool) {
+        const double* __restrict__ params, int layer, uint64_t* pool, unsigned long long resident_bytes) {
   constexpr int NW = BLOCK / 32;
   constexpr unsigned long long TILE = (unsigned long long)BLOCK * ITEMS;
   __shared__ unsigned s_base[ITEMS * NW + 1];
   __shared__ unsigned long long s_red[2 * NW];
+  extern __shared__ __align__(16) uint64_t s_region[];  // resident_bytes of dynamic shared memory
   BInst& I = insts[blockIdx.x];
   if (I.err) return;
   const unsigned end = (layer < 0 || (unsigned)layer >= I.n_layers)
@@ -309,7 +314,26 @@ k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ 
                            : min(I.op_end, layer_ends[I.layer_off + (unsigned)layer]);
   unsigned pc = I.pc;
   if (pc >= end) return;
-  const Region<W> R = region_of<W>(pool, I);
+  // An instance whose whole region fits in the launch's dynamic shared memory runs there: its
+  // live terms are copied in, its pair table starts empty (a zero slot holds no epoch), and
+  // the terms go back to the pool at the end.  The op loop is the same code either way (R's
+  // arrays are generic pointers).  A region that does not fit runs from the pool.
+  const bool resident = 8ull * region_words(W, I.cap, I.tsize) <= resident_bytes;
+  const Region<W> R = resident ? region_at<W>(s_region, I.cap, I.tsize) : region_of<W>(pool, I);
+  if (resident) {
+    const Region<W> G = region_of<W>(pool, I);
+    const unsigned long long n0 = I.n;
+    for (unsigned long long i = threadIdx.x; i < n0; i += BLOCK) {
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        R.x[(size_t)w * R.cap + i] = G.x[(size_t)w * G.cap + i];
+        R.z[(size_t)w * R.cap + i] = G.z[(size_t)w * G.cap + i];
+      }
+      R.c[i] = G.c[i];
+    }
+    for (unsigned long long t = threadIdx.x; t < R.tsize; t += BLOCK) R.table[t] = 0ull;
+    __syncthreads();
+  }
   const double* __restrict__ P = params + I.param_off;
   const double thr = I.thr;
   const unsigned long long maxw = I.maxw;
@@ -528,6 +552,17 @@ k_batch(BInst* insts, const BOp* __restrict__ ops, const uint32_t* __restrict__ 
     ++pc;
   }
   __syncthreads();
+  if (resident) {  // the terms back to the pool (a failed op wrote nothing)
+    const Region<W> G = region_of<W>(pool, I);
+    for (unsigned long long i = threadIdx.x; i < N; i += BLOCK) {
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        G.x[(size_t)w * G.cap + i] = R.x[(size_t)w * R.cap + i];
+        G.z[(size_t)w * G.cap + i] = R.z[(size_t)w * R.cap + i];
+      }
+      G.c[i] = R.c[i];
+    }
+  }
   if (threadIdx.x == 0) {
     I.n = N;
     I.pc = pc;
@@ -660,6 +695,7 @@ struct ppvm_batch {
   uint64_t* d_init = nullptr;
   uint64_t* pool = nullptr;
   size_t pool_words = 0;
+  unsigned long long resident_bytes = 0;  // dynamic shared memory per CTA for resident instances
   double* d_out = nullptr;
   bool inputs_dirty = true;
   bool layout_dirty = true;
@@ -688,8 +724,14 @@ int batch_words(uint32_t n_max) {
 
 template <int W, int BLOCK, int ITEMS>
 cudaError_t launch_layer(ppvm_batch* b, int layer) {
-  k_batch<W, BLOCK, ITEMS><<<(unsigned)b->ninst, BLOCK, 0, b->stream>>>(b->d_inst, b->d_ops, b->d_lends,
-                                                                         b->d_params, layer, b->pool);
+  const size_t dyn = (size_t)b->resident_bytes;
+  if (dyn > 48 * 1024) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_batch<W, BLOCK, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+  }
+  k_batch<W, BLOCK, ITEMS><<<(unsigned)b->ninst, BLOCK, dyn, b->stream>>>(b->d_inst, b->d_ops, b->d_lends,
+                                                                           b->d_params, layer, b->pool, dyn);
   return cudaGetLastError();
 }
 
@@ -819,6 +861,34 @@ ppvm_status upload_inputs(ppvm_batch* b) {
   return PPVM_OK;
 }
 
+// Dynamic shared memory per CTA for resident instances: the largest region, when every
+// instance's region fits within what each CTA can hold while all of them stay resident
+// together (ceil(instances / SMs) CTAs per SM, 2 KB per CTA left to static shared memory and
+// the system); otherwise none.  A batch where only some instances fit runs all of them from
+// the pool: the shared memory taken by the small ones would shrink the L1 cache that the
+// large ones, which set the batch's time, read through.
+ppvm_status choose_resident(ppvm_batch* b) {
+  static const bool never = [] {  // PPVM_BATCH_RESIDENT=never: every instance from the pool
+    const char* e = std::getenv("PPVM_BATCH_RESIDENT");
+    return e && std::strcmp(e, "never") == 0;
+  }();
+  b->resident_bytes = 0;
+  if (never) return PPVM_OK;
+  int nsm = 0, per_sm_bytes = 0, optin = 0;
+  BCUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device));
+  BCUDA(cudaDeviceGetAttribute(&per_sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, b->device));
+  BCUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
+  const unsigned long long per_sm = (b->ninst + nsm - 1) / std::max(nsm, 1);
+  const unsigned long long share = (unsigned long long)per_sm_bytes / std::max<unsigned long long>(per_sm, 1);
+  unsigned long long budget = std::min<unsigned long long>((unsigned long long)optin, share);
+  budget = budget > 2048 ? ((budget - 2048) & ~15ull) : 0;
+  unsigned long long need = 0;
+  for (size_t i = 0; i < b->ninst; ++i)
+    need = std::max<unsigned long long>(need, 8ull * region_words(b->W, b->h_inst[i].cap, b->h_inst[i].tsize));
+  if (need <= budget) b->resident_bytes = need;
+  return PPVM_OK;
+}
+
 // Lays the pool out for the current capacities.  With keep, live terms move over.
 ppvm_status layout(ppvm_batch* b, bool keep) {
   std::vector<BInst> old(b->h_inst, b->h_inst + b->ninst);
@@ -833,6 +903,7 @@ ppvm_status layout(ppvm_batch* b, bool keep) {
     I.epoch = 0;
   }
   const size_t bytes = sizeof(uint64_t) * std::max<unsigned long long>(words, 1);
+  BTRY(choose_resident(b));
   BCUDA(cudaStreamSynchronize(b->stream));
   void* np = nullptr;
   BCUDA(ppvm::cache_malloc(&np, bytes));

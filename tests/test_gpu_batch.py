@@ -5,6 +5,9 @@ terms in the same order (IndexMap order), every coefficient bit for bit, and the
 count entering every gate (term-gate updates).  overlap_with_zero is compared to 1e-10.
 """
 
+import os
+import sys
+
 import numpy as np
 import pytest
 
@@ -167,3 +170,17 @@ def test_bulk_setter_names_the_failing_instance():
     b = PauliSumBatch([good, good])
     b.run()
     check_batch(b)
+
+
+def test_batches_from_the_pool_match_the_oracle():
+    # small instances run resident in shared memory by default; the same cases again with
+    # PPVM_BATCH_RESIDENT=never (read once per process, so in a child process) run every
+    # instance from the device pool
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, PPVM_BATCH_RESIDENT="never")
+    r = subprocess.run([sys.executable, "-m", "pytest", "tests/test_gpu_batch.py", "-m", "gpu", "-x", "-q",
+                        "-k", "not from_the_pool"], cwd=root, env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert " passed" in r.stdout
