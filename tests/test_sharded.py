@@ -148,12 +148,12 @@ def _rank_main(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
-def test_two_ranks_hold_the_unsharded_term_set(tmp_path):
+@pytest.mark.parametrize("world", [2, 3])
+def test_ranks_hold_the_unsharded_term_set(tmp_path, world):
     import torch.multiprocessing as mp
 
     from oracle.pyoracle import OracleSum
 
-    world = 2
     mp.spawn(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
     res = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(world)]
     for name, n, word, ops, thr, maxw, ca in _circuits():
