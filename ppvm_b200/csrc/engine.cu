@@ -312,14 +312,16 @@ unsigned long long run_scratch_min_groups() {
   return v;
 }
 
-// k_run_groups' tiled mode (one look-back per tile of groups): 0 chooses per run (tiled when
-// most groups hold a single member), 1 always, 2 never.  PPVM_RUN_TILED=always|never
-// overrides the choice; the tests run the fused-run cases both ways.
+// The group mode of k_run_groups: 0 chosen per run (many single-member groups: one group per
+// lane; otherwise one group per warp), 1 tiles of groups per block, 2 one group per warp, 3 one
+// group per lane.  PPVM_RUN_GROUP_MODE=tiled|warp|lanes forces one; the tests run the
+// fused-run cases in each.
 unsigned run_tile_mode() {
   static const unsigned v = [] {
-    const char* e = std::getenv("PPVM_RUN_TILED");
-    if (e && std::strcmp(e, "always") == 0) return 1u;
-    if (e && std::strcmp(e, "never") == 0) return 2u;
+    const char* e = std::getenv("PPVM_RUN_GROUP_MODE");
+    if (e && std::strcmp(e, "tiled") == 0) return 1u;
+    if (e && std::strcmp(e, "warp") == 0) return 2u;
+    if (e && std::strcmp(e, "lanes") == 0) return 3u;
     return 0u;
   }();
   return v;

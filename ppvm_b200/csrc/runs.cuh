@@ -610,12 +610,179 @@ __device__ __forceinline__ void group_write(const RunGroup<W>& G, Planes D, unsi
   }
 }
 
-// The groups of a run, in one of three modes chosen per launch (the same in every block):
+// ---- lane mode: one group per lane ------------------------------------------------------
+constexpr int kRunLaneK = 3;  // groups of up to 3 coordinates (8 slots) run on one lane
+
+// A small group on one lane: its slots in registers (slot c at coef[c], existence bit c of
+// ex), its key and coordinate qubits, the gates of its coordinates in run order.
+template <int W>
+struct LaneGroup {
+  uint64_t v[W], f0[W];
+  uint16_t pos[kRunLaneK];  // qubit of coordinate bit t (ascending)
+  uint8_t ord[kRunLaneK];   // coordinate bits in gate order
+  unsigned k;
+  bool wok;
+  double coef[1 << kRunLaneK];
+  unsigned ex;
+};
+
+// Loads group g's key on this lane: v, f0, its coordinates; false when it has more than
+// kRunLaneK coordinates (the warp runs it instead).
+template <int W>
+__device__ __forceinline__ bool lane_key(LaneGroup<W>& G, unsigned long long g, const RunDesc* rd,
+                                         const RunScratch& R, const uint16_t* s_gidx, bool wcap,
+                                         unsigned long long maxw) {
+  const uint64_t* gk = R.gkey + g * 2 * W;
+  unsigned k = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    G.v[w] = gk[w];
+    G.f0[w] = gk[W + w];
+    k += __popcll(G.v[w] & rd->Q[w]);
+  }
+  G.k = k;
+  if (k > (unsigned)kRunLaneK) return false;
+  unsigned t = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    uint64_t m = G.v[w] & rd->Q[w];
+    while (m) {
+      const int b = __ffsll((long long)m) - 1;
+      m &= m - 1;
+      if (t < (unsigned)kRunLaneK) G.pos[t] = (uint16_t)(w * 64 + b);
+      ++t;
+    }
+  }
+  // coordinate bits by gate position (insertion sort of at most 3)
+  for (unsigned a = 0; a < k; ++a) G.ord[a] = (uint8_t)a;
+  for (unsigned a = 1; a < k; ++a)
+    for (unsigned b = a; b > 0 && s_gidx[G.pos[G.ord[b - 1]]] > s_gidx[G.pos[G.ord[b]]]; --b) {
+      const uint8_t tmp = G.ord[b - 1];
+      G.ord[b - 1] = G.ord[b];
+      G.ord[b] = tmp;
+    }
+  G.wok = true;
+  if (wcap) {
+    unsigned wt = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) wt += __popcll(G.v[w] | G.f0[w]);
+    G.wok = wt <= maxw;
+  }
+  return true;
+}
+
+// The members and the butterfly of a small group on its lane, the same arithmetic in the same
+// gate order as group_butterfly; children made per gate go to s_created.
+template <int W>
+__device__ __forceinline__ void lane_run(LaneGroup<W>& G, unsigned long long g, uint32_t cls, const RunScratch& R,
+                                         const uint16_t* s_gidx, const double* s_cs, const double* s_sn,
+                                         unsigned long long* s_created) {
+  constexpr int SZ = 1 << kRunLaneK;
+  const uint32_t start = R.g_start[g], cnt = R.g_cnt[g];
+  G.ex = 0;
+#pragma unroll
+  for (int c = 0; c < SZ; ++c) G.coef[c] = 0.0;
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const unsigned c = R.mcoord[start + m];
+    const double v = R.mcoef[start + m];
+#pragma unroll
+    for (int e = 0; e < SZ; ++e)
+      if (e == (int)c) G.coef[e] = v;
+    G.ex |= 1u << c;
+  }
+  const double eps_a = cls == 0 ? 1.0 : -1.0, eps_b = -eps_a;
+  for (unsigned r = 0; r < G.k; ++r) {
+    const unsigned t = G.ord[r];
+    const unsigned j = s_gidx[G.pos[t]];
+    const unsigned bit = 1u << t;
+    const double cs = s_cs[j], sn = s_sn[j];
+    unsigned made = 0;
+#pragma unroll
+    for (int a = 0; a < SZ; ++a) {
+      if ((a & (int)bit) || a >= (1 << G.k)) continue;
+      const int b = a | (int)bit;
+      double ca = 0.0, cb = 0.0;
+#pragma unroll
+      for (int e = 0; e < SZ; ++e) {  // registers only: slots picked by compile-time index
+        if (e == a) ca = G.coef[e];
+        if (e == b) cb = G.coef[e];
+      }
+      const bool ea = (G.ex >> a) & 1u, eb = (G.ex >> b) & 1u;
+      double na = ca, nb = cb;
+      if (ea && eb) {
+        na = __dadd_rn(__dmul_rn(ca, cs), __dmul_rn(cb, eps_b * sn));
+        nb = __dadd_rn(__dmul_rn(cb, cs), __dmul_rn(ca, eps_a * sn));
+      } else if (ea) {
+        na = __dmul_rn(ca, cs);
+        nb = __dmul_rn(ca, eps_a * sn);
+        G.ex |= 1u << b;
+        ++made;
+      } else if (eb) {
+        nb = __dmul_rn(cb, cs);
+        na = __dmul_rn(cb, eps_b * sn);
+        G.ex |= 1u << a;
+        ++made;
+      }
+#pragma unroll
+      for (int e = 0; e < SZ; ++e) {
+        if (e == a) G.coef[e] = na;
+        if (e == b) G.coef[e] = nb;
+      }
+    }
+    if (made) atomicAdd(&s_created[j], (unsigned long long)made);
+  }
+}
+
+// Whether slot c of a small group is written (it exists and passes the run's TRUNCATE).
+template <int W>
+__device__ __forceinline__ bool lane_keep(const LaneGroup<W>& G, int c, int trunc, double thr) {
+  if (!((G.ex >> c) & 1u)) return false;
+  if (!trunc) return true;
+  double v = 0.0;
+#pragma unroll
+  for (int e = 0; e < (1 << kRunLaneK); ++e)
+    if (e == c) v = G.coef[e];
+  return G.wok && !(fabs(v) < thr);
+}
+
+// Writes a small group's survivors, in coordinate order, to D from index out on.
+template <int W>
+__device__ __forceinline__ void lane_write(const LaneGroup<W>& G, Planes D, unsigned long long out, uint32_t cls,
+                                           int trunc, double thr) {
+#pragma unroll
+  for (int c = 0; c < (1 << kRunLaneK); ++c) {
+    if (c >= (1 << G.k) || !lane_keep<W>(G, c, trunc, thr)) continue;
+    if (out < D.cap) {
+      uint64_t f[W], x[W], z[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w) f[w] = G.f0[w];
+      for (unsigned t = 0; t < G.k; ++t)
+        if ((c >> t) & 1) {
+          const unsigned q = G.pos[t];
+#pragma unroll
+          for (int w = 0; w < W; ++w)
+            if (w == (int)(q >> 6)) f[w] |= 1ull << (q & 63);
+        }
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        x[w] = cls == 0 ? f[w] : G.v[w];
+        z[w] = cls == 0 ? G.v[w] : f[w];
+      }
+      store_key<W>(D, out, x, z);
+      D.c[out] = G.coef[c];
+    }
+    ++out;
+  }
+}
+
+// The groups of a run, in one of four modes chosen per launch (the same in every block):
+// - one group per lane (at least kRunTileMinGroups groups of fewer than 1.5 members on
+//   average, the usual case; in look-back or scratch placement): see the lane-mode branch;
 // - one group per warp, taken by ticket (groups of several members): the warp runs the
 //   butterfly, counts the survivors, finds the group's output offset by a warp look-back over
 //   the lower-numbered groups, and writes;
-// - tiles of kRunTileGroups groups per block (at least kRunTileMinGroups groups of fewer
-//   than 1.5 members on average, or tile_mode 1): warp w takes the tile's groups w,
+// - tiles of kRunTileGroups groups per block (tile_mode 1 only; lane mode replaced it in the
+//   automatic choice): warp w takes the tile's groups w,
 //   w + kRunWarps, ...; the warps run every butterfly and count, a block scan orders the
 //   counts, one decoupled look-back places the tile after all lower tiles, and the warps then
 //   write, each warp's last group straight from its slots and the others after running their
@@ -665,13 +832,87 @@ k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   unsigned* ex = s_ex[warp];
   uint8_t* ord = s_ord[warp];
   // Many mostly single-member groups (runs over sums whose terms rarely share a group; their
-  // butterflies are short) go in block tiles: there the per-group look-backs cost more than
-  // running the butterflies twice.  Groups of several members (long butterflies), and runs
-  // of few groups (which tiles would spread over too few warps), go one per warp.
-  // tile_mode 1 or 2 forces either.  The choice is the same in every block.
+  // butterflies are short) go 32 to a warp, one per lane.  Groups of several members go one
+  // per warp.  tile_mode forces a mode (1 tiles, 2 one group per warp, 3 lanes); the choice
+  // is the same in every block.
   const unsigned long long members = ld_volatile(&ctrl->n_side);
-  const bool tiled = !scratch && (tile_mode == 1 || (tile_mode == 0 && ngroups >= kRunTileMinGroups &&
-                                                     2 * members < 3 * ngroups));
+  const bool singles = ngroups >= kRunTileMinGroups && 2 * members < 3 * ngroups;
+  const bool lanes = tile_mode == 3 || (tile_mode == 0 && singles);
+  const bool tiled = !lanes && !scratch && tile_mode == 1;
+  if (lanes) {
+    // lane mode: a warp takes 32 consecutive groups by one ticket.  A group of at most
+    // kRunLaneK coordinates runs on its lane alone; a larger one is run by the whole warp.
+    // One warp scan and one look-back (or one scratch counter step) place the 32 groups, and
+    // the warp runs its large groups again to write them.
+    const unsigned long long ntiles = (ngroups + 31) / 32;
+    for (;;) {
+      unsigned long long t = 0;
+      if (lane == 0) t = atomicAdd(&ctrl->tickets[2], 1ull);
+      t = __shfl_sync(kFull, t, 0);
+      if (t >= ntiles) break;
+      const unsigned long long g = t * 32 + lane;
+      const bool valid = g < ngroups;
+      LaneGroup<W> LG;
+      bool small = false;
+      unsigned mine = 0;
+      if (valid) {
+        small = lane_key<W>(LG, g, rd, R, s_gidx, wcap, maxw);
+        if (small) {
+          lane_run<W>(LG, g, cls, R, s_gidx, s_cs, s_sn, s_created);
+#pragma unroll
+          for (int c = 0; c < (1 << kRunLaneK); ++c)
+            if (c < (1 << LG.k)) mine += lane_keep<W>(LG, c, trunc, thr);
+        }
+      }
+      const unsigned big = __ballot_sync(kFull, valid && !small);
+      for (unsigned bb = big; bb; bb &= bb - 1) {
+        const unsigned l = (unsigned)(__ffs(bb) - 1);
+        RunGroup<W> G;
+        group_load<W>(G, t * 32 + l, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
+        group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, s_created);
+        const unsigned m = group_count<W>(G, coef, ex, trunc, thr);
+        if (lane == l) mine = m;
+        __syncwarp();
+      }
+      unsigned incl = mine;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= (unsigned)o) incl += v;
+      }
+      const unsigned total = __shfl_sync(kFull, incl, 31);
+      const unsigned pre = incl - mine;
+      unsigned long long base;
+      if (scratch) {
+        unsigned long long b0 = 0;
+        if (lane == 0) b0 = atomicAdd(&ctrl->scr_top, (unsigned long long)total);
+        base = __shfl_sync(kFull, b0, 0);
+        if (valid) {
+          const unsigned long long at = base + pre;
+          R.g_rep[g] = (uint32_t)(at < 0xFFFFFFFFull ? at : 0xFFFFFFFFull);  // scratch offset (< 2^32)
+          R.g_fill[g] = mine;                                                  // survivors
+        }
+      } else {
+        base = ubase + warp_lookback(ts, t, total, epoch, ctrl, op);
+      }
+      const Planes D = scratch ? S : O;
+      if (valid && small) lane_write<W>(LG, D, base + pre, cls, trunc, thr);
+      for (unsigned bb = big; bb; bb &= bb - 1) {
+        const unsigned l = (unsigned)(__ffs(bb) - 1);
+        const unsigned long long at = base + __shfl_sync(kFull, pre, l);
+        __syncwarp();
+        RunGroup<W> G;
+        group_load<W>(G, t * 32 + l, rd, R, s_gidx, ord, coef, ex, wcap, maxw);
+        group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, nullptr);
+        group_write<W>(G, D, at, cls, coef, ex, trunc, thr);
+      }
+      if (!scratch && t == ntiles - 1 && lane == 0) {
+        ctrl->cap_needed = base + total;
+        if (base + total > O.cap) set_err(ctrl, kErrCapacity, op);
+      }
+      __syncwarp();
+    }
+  } else
   if (!tiled) {
     for (;;) {
       unsigned long long g = 0;
