@@ -1052,7 +1052,7 @@ struct K {
     if (allow) {
       ProfScope ps(s, F_RUN_PLACE, op0, L);
       launch(k_run_place<W, 256, 2>, grid_for(nub, 512, 4), 256, 0, s->stream,
-          S, O, s->d_ctrl, s->R, scratch_min, s->tstate, s->next_tile_epoch(), op0);
+          S, O, s->d_ctrl, s->R, scratch_min, s->tstate, s->next_tile_epoch(), op0, run_tile_mode());
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);

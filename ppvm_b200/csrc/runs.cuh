@@ -775,9 +775,16 @@ __device__ __forceinline__ void lane_write(const LaneGroup<W>& G, Planes D, unsi
   }
 }
 
+// Whether a run's groups go one per lane: forced (tile_mode 3), or chosen for many groups of
+// mostly one member.  Lane mode places its 32-group tiles by look-back, never in scratch
+// mode, so k_run_place makes the same decision to stand aside.
+__device__ __forceinline__ bool run_lanes(unsigned long long ngroups, unsigned long long members, unsigned tile_mode) {
+  return tile_mode == 3 || (tile_mode == 0 && ngroups >= kRunTileMinGroups && 2 * members < 3 * ngroups);
+}
+
 // The groups of a run, in one of four modes chosen per launch (the same in every block):
 // - one group per lane (at least kRunTileMinGroups groups of fewer than 1.5 members on
-//   average, the usual case; in look-back or scratch placement): see the lane-mode branch;
+//   average; placed by look-back at any group count): see the lane-mode branch;
 // - one group per warp, taken by ticket (groups of several members): the warp runs the
 //   butterfly, counts the survivors, finds the group's output offset by a warp look-back over
 //   the lower-numbered groups, and writes;
@@ -789,9 +796,9 @@ __device__ __forceinline__ void lane_write(const LaneGroup<W>& G, Planes D, unsi
 //   butterflies again (the same arithmetic in the same order, so the same coefficients).  One
 //   look-back per tile instead of per group; the second butterfly costs less than the
 //   look-backs it saves only when the butterflies are short;
-// - scratch mode (many groups): one group per warp, its survivors written at once to the
-//   scratch planes S wherever a counter puts them; k_run_place then moves every group's
-//   block to its place in O.
+// - scratch mode (many groups, when not in lane mode): one group per warp, its survivors
+//   written at once to the scratch planes S wherever a counter puts them; k_run_place then
+//   moves every group's block to its place in O.
 // Every mode writes the same terms in the same order: groups by number, members by
 // coordinate.
 template <int W>
@@ -824,25 +831,20 @@ k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
   if (s_err) return;
   const unsigned long long ngroups = ld_volatile(&ctrl->n_pairs);
   const unsigned long long ubase = ld_volatile(&ctrl->n_s);  // untouched survivors go first
-  const bool scratch = ngroups >= scratch_min;               // the same in every block
+  const unsigned long long members = ld_volatile(&ctrl->n_side);
+  const bool lanes = run_lanes(ngroups, members, tile_mode);  // the same in every block
+  const bool scratch = !lanes && ngroups >= scratch_min;
   const uint32_t cls = rd->cls;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool wcap = maxw != ~0ull;
   double* coef = s_coef[warp];
   unsigned* ex = s_ex[warp];
   uint8_t* ord = s_ord[warp];
-  // Many mostly single-member groups (runs over sums whose terms rarely share a group; their
-  // butterflies are short) go 32 to a warp, one per lane.  Groups of several members go one
-  // per warp.  tile_mode forces a mode (1 tiles, 2 one group per warp, 3 lanes); the choice
-  // is the same in every block.
-  const unsigned long long members = ld_volatile(&ctrl->n_side);
-  const bool singles = ngroups >= kRunTileMinGroups && 2 * members < 3 * ngroups;
-  const bool lanes = tile_mode == 3 || (tile_mode == 0 && singles);
   const bool tiled = !lanes && !scratch && tile_mode == 1;
   if (lanes) {
     // lane mode: a warp takes 32 consecutive groups by one ticket.  A group of at most
     // kRunLaneK coordinates runs on its lane alone; a larger one is run by the whole warp.
-    // One warp scan and one look-back (or one scratch counter step) place the 32 groups, and
+    // One warp scan and one look-back place the 32 groups, and
     // the warp runs its large groups again to write them.
     const unsigned long long ntiles = (ngroups + 31) / 32;
     for (;;) {
@@ -882,20 +884,8 @@ k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
       }
       const unsigned total = __shfl_sync(kFull, incl, 31);
       const unsigned pre = incl - mine;
-      unsigned long long base;
-      if (scratch) {
-        unsigned long long b0 = 0;
-        if (lane == 0) b0 = atomicAdd(&ctrl->scr_top, (unsigned long long)total);
-        base = __shfl_sync(kFull, b0, 0);
-        if (valid) {
-          const unsigned long long at = base + pre;
-          R.g_rep[g] = (uint32_t)(at < 0xFFFFFFFFull ? at : 0xFFFFFFFFull);  // scratch offset (< 2^32)
-          R.g_fill[g] = mine;                                                  // survivors
-        }
-      } else {
-        base = ubase + warp_lookback(ts, t, total, epoch, ctrl, op);
-      }
-      const Planes D = scratch ? S : O;
+      const unsigned long long base = ubase + warp_lookback(ts, t, total, epoch, ctrl, op);
+      const Planes D = O;
       if (valid && small) lane_write<W>(LG, D, base + pre, cls, trunc, thr);
       for (unsigned bb = big; bb; bb &= bb - 1) {
         const unsigned l = (unsigned)(__ffs(bb) - 1);
@@ -906,7 +896,7 @@ k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
         group_butterfly<W>(G, cls, ord, s_gidx, s_cs, s_sn, coef, ex, nullptr);
         group_write<W>(G, D, at, cls, coef, ex, trunc, thr);
       }
-      if (!scratch && t == ntiles - 1 && lane == 0) {
+      if (t == ntiles - 1 && lane == 0) {
         ctrl->cap_needed = base + total;
         if (base + total > O.cap) set_err(ctrl, kErrCapacity, op);
       }
@@ -1005,7 +995,7 @@ k_run_groups(Planes O, Planes S, Ctrl* ctrl, const RunDesc* rd, RunScratch R, in
 template <int W, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_run_place(Planes S, Planes O, Ctrl* ctrl, RunScratch R, unsigned long long scratch_min, unsigned long long* ts,
-            unsigned epoch, int op) {
+            unsigned epoch, int op, unsigned tile_mode) {
   pdl_wait();
   constexpr int NW = BLOCK / 32;
   constexpr int TILE = BLOCK * ITEMS;
@@ -1017,7 +1007,8 @@ k_run_place(Planes S, Planes O, Ctrl* ctrl, RunScratch R, unsigned long long scr
   __shared__ int s_skip;
   if (threadIdx.x == 0) {
     const unsigned long long ng = ld_volatile(&ctrl->n_pairs);
-    s_skip = ld_volatile_int(&ctrl->err) || ng == 0 || ng < scratch_min;
+    s_skip = ld_volatile_int(&ctrl->err) || ng == 0 || ng < scratch_min ||
+             run_lanes(ng, ld_volatile(&ctrl->n_side), tile_mode);
   }
   __syncthreads();
   if (s_skip) return;  // the same in every block (look-back mode, or an earlier error)
