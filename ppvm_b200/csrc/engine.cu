@@ -327,6 +327,19 @@ unsigned run_tile_mode() {
   return v;
 }
 
+// Chunk tables of the composed Clifford pass (one-word sums): 0 = by size and moved
+// generators, 1 = always (every warp with a moved bit takes them), 2 = never.
+// PPVM_TABLEAU_CHUNKS=always|never forces one; the tests run the tableau cases in each.
+unsigned tableau_chunk_mode() {
+  static const unsigned v = [] {
+    const char* e = std::getenv("PPVM_TABLEAU_CHUNKS");
+    if (e && std::strcmp(e, "always") == 0) return 1u;
+    if (e && std::strcmp(e, "never") == 0) return 2u;
+    return 0u;
+  }();
+  return v;
+}
+
 // Polls a look-back waits for its predecessors before it gives up with PPVM_ETIMEOUT.  0 (the
 // default) leaves the device's bound of 2^22 polls; PPVM_SPIN_LIMIT overrides it, read once
 // per process (the timeout test sets a few polls, so that a multi-tile look-back gives up).
@@ -1069,7 +1082,16 @@ struct K {
     const void* d_ph = nullptr;
     PPVM_TRY(stage_put(s, t.rows.data(), t.rows.size() * sizeof(uint64_t), &d_rows));
     PPVM_TRY(stage_put(s, t.ph.data(), t.ph.size(), &d_ph));
-    const size_t smem = t.rows.size() * sizeof(uint64_t) + t.ph.size();
+    const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
+    // one-word sums of many terms through a run that moves many generators: chunk tables
+    int chunk_min = -1;
+    if constexpr (W == 1) {
+      const unsigned mode = tableau_chunk_mode();
+      const int moved = __builtin_popcountll(t.tp.Tx[0]) + __builtin_popcountll(t.tp.Tz[0]);
+      if (mode == 1 && moved > 0) chunk_min = 0;
+      else if (mode == 0 && nub >= kTabChunkMinTerms && moved >= kTabChunkMinMoved) chunk_min = kTabChunkMinBits;
+    }
+    const size_t smem = t.rows.size() * sizeof(uint64_t) + t.ph.size() + (chunk_min >= 0 ? kTabChunkSmem : 0);
     if (smem > kTabMaxSmem) return fail(PPVM_EINVAL, "internal: tableau exceeds shared memory");
     static unsigned long long attr_set = 0;  // one bit per device
     if (!((attr_set >> s->device) & 1ull)) {
@@ -1077,14 +1099,15 @@ struct K {
                                     (int)kTabMaxSmem));
       attr_set |= 1ull << s->device;
     }
-    const int bps = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / (smem + 4096)));
-    const unsigned long long nub = std::max<unsigned long long>(s->n_ub, 1);
+    // blocks per SM: with the tables, as many as 227 KB of shared memory hold (3)
+    const int bps = chunk_min >= 0 ? (int)std::max<size_t>(1, std::min<size_t>(4, (227 * 1024) / (smem + 2048)))
+                                   : (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / (smem + 4096)));
     {
       ProfScope ps(s, F_TABLEAU, op0, nops, trunc_op);
       launch(k_tableau<W, kTabBlock, ITEMS>, grid_for(nub, (unsigned long long)kTabBlock * ITEMS, bps), kTabBlock, smem, s->stream,
           P, O, s->d_ctrl, t.tp, static_cast<const uint64_t*>(d_rows), static_cast<const uint8_t*>(d_ph),
           trunc_op >= 0 ? 1 : 0, s->thr, s->maxw, s->tstate, s->next_tile_epoch(), op0, nops, trunc_op,
-          s->d_log);  // its last block publishes the count
+          s->d_log, chunk_min);  // its last block publishes the count
     }
     std::swap(s->planes, s->alt);
     s->swaps.push_back(op0);

@@ -161,26 +161,123 @@ __device__ __forceinline__ unsigned tab_map(const uint64_t* rows, const uint8_t*
   return (p - hw) & 3u;
 }
 
+// ---- chunk tables (one machine word, n <= 64) ----------------------------------------------
+// tab_map costs one image per moved bit, up to 128 for a heavy 64-qubit term.  With one word
+// the block can instead tabulate, for each 4-qubit chunk c, the images of all 256 sub-words
+// X^{x_c} Z^{z_c} (16 tables, 64 KB of shared memory), and a term maps with 16 lookups
+// whatever its weight.  The chunks' factors act on disjoint qubits and commute, so
+//   X^x Z^z = prod_c X^{x_c} Z^{z_c}   and   f(X^x Z^z) = prod_c f(X^{x_c} Z^{z_c})
+// exactly, phases included: the image is the one tab_map computes.  A warp takes the tables
+// when one of its terms has more than chunk_min moved bits.
+constexpr int kTabChunks = 16;                 // 4 qubits each
+constexpr int kTabChunkEntries = 256;          // index: x nibble | z nibble << 4
+constexpr size_t kTabChunkSmem = (size_t)kTabChunks * kTabChunkEntries * (2 * sizeof(uint64_t) + 1);
+constexpr int kTabChunkMinBits = 12;           // per warp: tables above this many moved bits
+constexpr unsigned long long kTabChunkMinTerms = 1ull << 15;  // host: build them from here on
+constexpr int kTabChunkMinMoved = 32;          // host: and when the run moves this many generators
+
+// The image of X_q (s = 0) or Z_q (s = 1) multiplied onto i^p X^u Z^v from the right.
+__device__ __forceinline__ void tab_mul_gen(const uint64_t* rows, const uint8_t* ph, uint64_t T, int q, int s,
+                                            uint64_t& u, uint64_t& v, unsigned& p) {
+  uint64_t a, b;
+  unsigned e;
+  if ((T >> q) & 1ull) {
+    const unsigned row = 2u * (unsigned)__popcll(T & ((1ull << q) - 1ull)) + (unsigned)s;
+    a = rows[2 * row];
+    b = rows[2 * row + 1];
+    e = ph[row];
+  } else {  // untouched qubit: the generator itself
+    a = s ? 0ull : 1ull << q;
+    b = s ? 1ull << q : 0ull;
+    e = 0;
+  }
+  p += e + 2u * (unsigned)__popcll(v & a);
+  u ^= a;
+  v ^= b;
+}
+
+// Fills the 16 chunk tables: thread (c, x nibble) forms f(X^{x_c}), then walks the 16 z nibbles
+// in Gray-code order, one image product per entry.  Dropping Z_q again multiplies by f(Z_q),
+// which is exact: the Z images commute and each squares to the identity.
+__device__ inline void tab_build_chunks(const uint64_t* rows, const uint8_t* ph, uint64_t T, uint64_t* tab,
+                                        uint8_t* tph) {
+  for (unsigned t = threadIdx.x; t < (unsigned)kTabChunks * 16u; t += blockDim.x) {
+    const int c = (int)(t >> 4);
+    const unsigned xv = t & 15u;
+    uint64_t u = 0, v = 0;
+    unsigned p = 0;
+    for (int j = 0; j < 4; ++j)
+      if ((xv >> j) & 1u) tab_mul_gen(rows, ph, T, 4 * c + j, 0, u, v, p);
+    unsigned idx = (unsigned)c * kTabChunkEntries + xv;
+    tab[2 * idx] = u;
+    tab[2 * idx + 1] = v;
+    tph[idx] = (uint8_t)(p & 3u);
+    unsigned g = 0;
+    for (unsigned k = 1; k < 16; ++k) {
+      const int j = __ffs((int)k) - 1;
+      g ^= 1u << j;
+      tab_mul_gen(rows, ph, T, 4 * c + j, 1, u, v, p);
+      idx = (unsigned)c * kTabChunkEntries + (xv | (g << 4));
+      tab[2 * idx] = u;
+      tab[2 * idx + 1] = v;
+      tph[idx] = (uint8_t)(p & 3u);
+    }
+  }
+}
+
+// tab_map for one word through the chunk tables; same contract.
+__device__ __forceinline__ unsigned tab_map_chunks(const uint64_t* tab, const uint8_t* tph, uint64_t x, uint64_t z,
+                                                   uint64_t& ox, uint64_t& oz) {
+  unsigned p = (unsigned)__popcll(x & z);
+  uint64_t u = 0, v = 0;
+  const ulonglong2* t2 = reinterpret_cast<const ulonglong2*>(tab);
+#pragma unroll
+  for (int c = 0; c < kTabChunks; ++c) {
+    const unsigned idx = (unsigned)c * kTabChunkEntries + (unsigned)((x >> (4 * c)) & 15ull) +
+                         ((unsigned)((z >> (4 * c)) & 15ull) << 4);
+    const ulonglong2 e = t2[idx];
+    p += tph[idx] + 2u * (unsigned)__popcll(v & e.x);
+    u ^= e.x;
+    v ^= e.y;
+  }
+  ox = u;
+  oz = v;
+  return (p - (unsigned)__popcll(u & v)) & 3u;
+}
+
 // Maps every live term through the run; with trunc, drops what the strategy drops.  Survivors
 // go to O in input order; the last block to finish publishes their count (and the log of the
-// fused TRUNCATE, trunc_op).
+// fused TRUNCATE, trunc_op).  chunk_min >= 0 (one word only): the block builds the chunk
+// tables, and a warp maps through them when one of its terms has more than chunk_min moved
+// bits.  Dynamic shared memory: [chunk tables][rows][chunk phases][row phases], the chunk
+// parts only with chunk_min >= 0.
 template <int W, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
 k_tableau(Planes P, Planes O, Ctrl* ctrl, TabParams tp, const uint64_t* __restrict__ g_rows,
           const uint8_t* __restrict__ g_ph, int trunc, double thr, unsigned long long maxw,
-          unsigned long long* ts, unsigned epoch, int op0, int nops, int trunc_op, OpLog* log) {
+          unsigned long long* ts, unsigned epoch, int op0, int nops, int trunc_op, OpLog* log, int chunk_min) {
   pdl_wait();
-  extern __shared__ __align__(16) uint64_t s_rows[];  // nrows * 2W words, then nrows phase bytes
+  extern __shared__ __align__(16) uint64_t s_dyn[];
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_slot;
   __shared__ unsigned s_base[ITEMS * (BLOCK / 32) + 1];
   __shared__ int s_err;
-  uint8_t* s_ph = reinterpret_cast<uint8_t*>(s_rows + (size_t)tp.nrows * 2 * W);
+  const bool chunked = W == 1 && chunk_min >= 0;
+  uint64_t* s_tab = s_dyn;
+  uint64_t* s_rows = s_dyn + (chunked ? (size_t)kTabChunks * kTabChunkEntries * 2 : 0);
+  uint8_t* s_tph = reinterpret_cast<uint8_t*>(s_rows + (size_t)tp.nrows * 2 * W);
+  uint8_t* s_ph = s_tph + (chunked ? kTabChunks * kTabChunkEntries : 0);
   if (threadIdx.x == 0) s_err = ld_volatile_int(&ctrl->err);
   for (unsigned i = threadIdx.x; i < tp.nrows * 2 * W; i += BLOCK) s_rows[i] = g_rows[i];
   for (unsigned i = threadIdx.x; i < tp.nrows; i += BLOCK) s_ph[i] = g_ph[i];
   __syncthreads();
   if (s_err) return;
+  if constexpr (W == 1) {
+    if (chunked) {
+      tab_build_chunks(s_rows, s_ph, tp.T[0], s_tab, s_tph);
+      __syncthreads();
+    }
+  }
   const unsigned long long N = ld_volatile(&ctrl->n);
   constexpr unsigned long long TILE = (unsigned long long)BLOCK * ITEMS;
   const unsigned long long ntiles = (N + TILE - 1) / TILE;
@@ -207,11 +304,26 @@ k_tableau(Planes P, Planes O, Ctrl* ctrl, TabParams tp, const uint64_t* __restri
     for (int k = 0; k < ITEMS; ++k) {
       const unsigned long long i = base + (unsigned long long)k * BLOCK + threadIdx.x;
       bool keep = false;
+      uint64_t x[W], z[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w) x[w] = z[w] = 0ull;
+      if (i < N) load_key<W>(P, i, x, z);
+      [[maybe_unused]] bool use_tables = false;
+      if constexpr (W == 1) {
+        if (chunked) {  // warp-uniform: every lane of the block reaches each item
+          const int moved = __popcll(x[0] & tp.Tx[0]) + __popcll(z[0] & tp.Tz[0]);
+          use_tables = __any_sync(kFull, moved > chunk_min);
+        }
+      }
       if (i < N) {
-        uint64_t x[W], z[W];
-        load_key<W>(P, i, x, z);
         const double c = P.c[i];
-        const unsigned e = tab_map<W>(s_rows, s_ph, tp, x, z, ox[k], oz[k]);
+        unsigned e;
+        if constexpr (W == 1) {
+          e = use_tables ? tab_map_chunks(s_tab, s_tph, x[0], z[0], ox[k][0], oz[k][0])
+                         : tab_map<W>(s_rows, s_ph, tp, x, z, ox[k], oz[k]);
+        } else {
+          e = tab_map<W>(s_rows, s_ph, tp, x, z, ox[k], oz[k]);
+        }
         if (e & 1u) set_err(ctrl, kErrProbe, op0);  // not a Hermitian image: internal error
         oc[k] = (e == 2u) ? -c : c;
         keep = true;

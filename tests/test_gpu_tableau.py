@@ -116,3 +116,30 @@ def test_folded_segment_with_weight_cap_keeps_counts():
     from tests.test_gpu_parity import same_set
     same_set(g, o)
     assert np.array_equal(g.live_counts(), want)
+
+
+def heavy_and_light_terms(rng, n, k):
+    # light terms first (at most 3 non-identity qubits), heavy ones after: warps of light
+    # terms keep the per-generator product, warps of heavy ones take the chunk tables
+    terms = {}
+    while len(terms) < k // 2:
+        w = ["I"] * n
+        for q in rng.sample(range(n), rng.randrange(1, 4)):
+            w[q] = rng.choice("XYZ")
+        terms["".join(w)] = rng.uniform(-1, 1)
+    while len(terms) < k:
+        terms["".join(rng.choice("IXYZ") for _ in range(n))] = rng.uniform(-1, 1)
+    return list(terms.items())
+
+
+@pytest.mark.parametrize("n", [40, 64])
+def test_tableau_chunk_tables_on_large_one_word_sums(n):
+    # 40,000 terms of one word through runs that move most generators: the pass builds the
+    # chunk tables (from 2^15 terms on), and mixed warps choose per warp
+    rng = random.Random(100 + n)
+    terms = heavy_and_light_terms(rng, n, 40000)
+    ops = []
+    for _ in range(3):
+        ops += random_clifford_ops(rng, n, 120) + [G.truncate()]
+    run_both(terms, n, ops, thr=1e-4, maxw=None, clifford_angles=True, check_every=121)
+

@@ -130,3 +130,65 @@ def test_rejects_non_clifford_ops():
         clifford_tableau(4, [G.pauli_error(0, (0.1, 0.0, 0.0))])
     with pytest.raises(ValueError):
         clifford_tableau(4, [G.g1(G.H, 4)])
+
+
+def chunk_tables(ix, iz, sg, n):
+    """The one-word kernel's chunk tables: for each 4-qubit chunk c, the image of every
+    sub-word X^{x_c} Z^{z_c} (index x nibble | z nibble << 4) as (a, b, ph), image =
+    i^ph X^a Z^b, built per x nibble by a Gray-code walk over the z nibbles."""
+    def gen(q, kind):
+        if q >= n:  # beyond the register: the generator itself
+            return (1 << q, 0, 0) if kind == 0 else (0, 1 << q, 0)
+        row = 2 * q + kind
+        a, b = int(ix[row][0]), int(iz[row][0])
+        return a, b, (bin(a & b).count("1") + 2 * int(sg[row])) & 3
+
+    def mul(acc, img):
+        u, v, p = acc
+        a, b, e = img
+        return u ^ a, v ^ b, (p + e + 2 * bin(v & a).count("1")) & 3
+
+    tab = {}
+    for c in range(16):
+        for xv in range(16):
+            acc = (0, 0, 0)
+            for j in range(4):
+                if (xv >> j) & 1:
+                    acc = mul(acc, gen(4 * c + j, 0))
+            tab[c, xv] = acc
+            g = 0
+            for k in range(1, 16):
+                j = (k & -k).bit_length() - 1
+                g ^= 1 << j
+                acc = mul(acc, gen(4 * c + j, 1))
+                tab[c, xv | (g << 4)] = acc
+    return tab
+
+
+def apply_chunk_tables(tab, x, z):
+    x, z = int(x[0]), int(z[0])
+    u = v = 0
+    p = bin(x & z).count("1")
+    for c in range(16):
+        a, b, e = tab[c, ((x >> (4 * c)) & 15) | (((z >> (4 * c)) & 15) << 4)]
+        p += e + 2 * bin(v & a).count("1")
+        u ^= a
+        v ^= b
+    e = (p - bin(u & v).count("1")) & 3
+    assert e in (0, 2), "image is not Hermitian"
+    return u, v, (-1.0 if e == 2 else 1.0)
+
+
+@pytest.mark.parametrize("n,L,seed", [(5, 40, 21), (37, 150, 22), (64, 300, 23)])
+def test_chunk_tables_map_words_like_the_oracle(n, L, seed):
+    rng = random.Random(seed)
+    ops = random_clifford_ops(rng, n, L)
+    ix, iz, sg = clifford_tableau(n, ops)
+    tab = chunk_tables(ix, iz, sg, n)
+    for i in range(30):
+        word = "".join(rng.choice("IXYZ" if i % 2 else "IIIIIIIXYZ") for _ in range(n))
+        x0, z0 = G.parse_word(word, n)
+        u, v, sign = apply_chunk_tables(tab, x0, z0)
+        x, z, c = oracle_image(n, word, ops)
+        assert u == int(x[0]) and v == int(z[0])
+        assert sign == c
