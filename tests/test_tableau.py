@@ -179,7 +179,7 @@ def apply_chunk_tables(tab, x, z):
     return u, v, (-1.0 if e == 2 else 1.0)
 
 
-@pytest.mark.parametrize("n,L,seed", [(5, 40, 21), (37, 150, 22), (64, 300, 23)])
+@pytest.mark.parametrize("n,L,seed", [(1, 12, 24), (2, 20, 25), (5, 40, 21), (37, 150, 22), (64, 300, 23)])
 def test_chunk_tables_map_words_like_the_oracle(n, L, seed):
     rng = random.Random(seed)
     ops = random_clifford_ops(rng, n, L)
